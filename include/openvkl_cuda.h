@@ -1,0 +1,286 @@
+// Open VKL C API as exported by the B200 `cuda` device
+// (libopenvkl_device_cuda.so).
+//
+// Every declaration below re-states the signature of the reference interface
+// it replaces (Open VKL v2.0.2; file:line relative to its source tree) so an
+// application's existing sampling / traversal calls link against this library
+// unchanged.  Handles are the reference's {host, device} pair
+// (openvkl/include/openvkl/types.h:56-69).  Entry points marked EXTENSION have
+// no counterpart in the reference; they are the batched GPU forms of the
+// per-ray iterator calls and the precision / batching / learned patterns.
+//
+// Pointer arguments of the N / MN / batched calls may be host or device
+// memory; device memory is used in place, host memory is staged through the
+// device and the call synchronizes before returning.  All work runs on the
+// device's CUDA stream (vklDeviceSetVoidPtr(device, "cudaStream", stream)).
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define OPENVKL_CUDA_INTERFACE __declspec(dllexport)
+#else
+#define OPENVKL_CUDA_INTERFACE __attribute__((visibility("default")))
+#endif
+
+// ---------------------------------------------------------------------------
+// Types (openvkl/include/openvkl/types.h, VKLDataType.h, VKLFilter.h,
+// VKLFormat.h, VKLError.h, VKLLogLevel.h, data.h).
+// ---------------------------------------------------------------------------
+typedef struct { float x, y, z; } vkl_vec3f;
+typedef struct { int x, y, z; } vkl_vec3i;
+typedef struct { float lower, upper; } vkl_range1f;
+typedef struct { vkl_vec3f lower, upper; } vkl_box3f;
+typedef struct { float x[4], y[4], z[4]; } vkl_vvec3f4;
+typedef struct { float x[8], y[8], z[8]; } vkl_vvec3f8;
+typedef struct { float x[16], y[16], z[16]; } vkl_vvec3f16;
+typedef struct { float lower[4], upper[4]; } vkl_vrange1f4;
+typedef struct { float lower[8], upper[8]; } vkl_vrange1f8;
+typedef struct { float lower[16], upper[16]; } vkl_vrange1f16;
+
+typedef struct
+{
+  void *host;
+  void *device;
+} VKLObject;
+
+typedef struct VKLDeviceInternal *VKLDevice;
+typedef VKLObject VKLData;
+typedef VKLObject VKLVolume;
+typedef VKLObject VKLSampler;
+typedef VKLObject VKLIntervalIteratorContext;
+typedef VKLObject VKLHitIteratorContext;
+typedef VKLObject VKLObserver;
+typedef uint64_t VKLFeatureFlags;
+
+typedef enum
+{
+  VKL_DEVICE = 100, VKL_VOID_PTR = 200, VKL_BOOL = 250,
+  VKL_OBJECT = 0x8000000, VKL_DATA = 0x8000000 + 100, VKL_VOLUME,
+  VKL_STRING = 1500,
+  VKL_CHAR = 2000, VKL_UCHAR = 2500, VKL_SHORT = 3000, VKL_USHORT = 3500,
+  VKL_INT = 4000, VKL_VEC2I, VKL_VEC3I, VKL_VEC4I,
+  VKL_UINT = 4500, VKL_VEC2UI, VKL_VEC3UI, VKL_VEC4UI,
+  VKL_LONG = 5000, VKL_ULONG = 5550,
+  VKL_HALF = 5800,
+  VKL_FLOAT = 6000, VKL_VEC2F, VKL_VEC3F, VKL_VEC4F,
+  VKL_DOUBLE = 7000,
+  VKL_BOX1I = 8000, VKL_BOX2I, VKL_BOX3I, VKL_BOX4I,
+  VKL_BOX1F = 10000, VKL_BOX2F, VKL_BOX3F, VKL_BOX4F,
+  VKL_LINEAR2F = 12000, VKL_LINEAR3F, VKL_AFFINE2F, VKL_AFFINE3F,
+  VKL_UNKNOWN = 9999999
+} VKLDataType;
+
+typedef enum { VKL_DATA_DEFAULT = 0, VKL_DATA_SHARED_BUFFER = 1 } VKLDataCreationFlags;
+typedef enum { VKL_FILTER_NEAREST = 0, VKL_FILTER_LINEAR = 100, VKL_FILTER_CUBIC = 200 } VKLFilter;
+typedef enum { VKL_FORMAT_TILE = 0, VKL_FORMAT_DENSE_ZYX = 1, VKL_FORMAT_INVALID = 100 } VKLFormat;
+typedef enum
+{
+  VKL_NO_ERROR = 0, VKL_UNKNOWN_ERROR = 1, VKL_INVALID_ARGUMENT = 2,
+  VKL_INVALID_OPERATION = 3, VKL_OUT_OF_MEMORY = 4, VKL_UNSUPPORTED_CPU = 5
+} VKLError;
+typedef enum
+{
+  VKL_LOG_DEBUG = 1, VKL_LOG_INFO = 2, VKL_LOG_WARNING = 3, VKL_LOG_ERROR = 4,
+  VKL_LOG_NONE = 5
+} VKLLogLevel;
+
+// VKLInterval / VKLHit (openvkl/devices/cpu/include/openvkl/device/openvkl.h:
+// 174-180, :315-320).
+typedef struct
+{
+  vkl_range1f tRange;
+  vkl_range1f valueRange;
+  float nominalDeltaT;
+} VKLInterval;
+
+typedef struct
+{
+  float t;
+  float sample;
+  float epsilon;
+} VKLHit;
+
+typedef struct IntervalIterator *VKLIntervalIterator;
+typedef struct HitIterator *VKLHitIterator;
+
+typedef void (*VKLLogCallback)(void *userData, const char *message);
+typedef void (*VKLErrorCallback)(void *userData, VKLError error, const char *message);
+
+// ---------------------------------------------------------------------------
+// Device (openvkl/include/openvkl/device.h:15-75; init
+// devices/cpu/include/openvkl/device/openvkl.h:23).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE void vklInit(void);
+OPENVKL_CUDA_INTERFACE VKLDevice vklNewDevice(const char *deviceName);
+OPENVKL_CUDA_INTERFACE void vklDeviceSetLogCallback(VKLDevice, VKLLogCallback, void *userData);
+OPENVKL_CUDA_INTERFACE void vklDeviceSetErrorCallback(VKLDevice, VKLErrorCallback, void *userData);
+OPENVKL_CUDA_INTERFACE void vklDeviceSetInt(VKLDevice, const char *name, int x);
+OPENVKL_CUDA_INTERFACE void vklDeviceSetString(VKLDevice, const char *name, const char *s);
+OPENVKL_CUDA_INTERFACE void vklDeviceSetVoidPtr(VKLDevice, const char *name, void *v);
+OPENVKL_CUDA_INTERFACE void vklCommitDevice(VKLDevice);
+OPENVKL_CUDA_INTERFACE VKLError vklDeviceGetLastErrorCode(VKLDevice);
+OPENVKL_CUDA_INTERFACE const char *vklDeviceGetLastErrorMsg(VKLDevice);
+OPENVKL_CUDA_INTERFACE int vklGetNativeSIMDWidth(VKLDevice);
+OPENVKL_CUDA_INTERFACE void vklCommit(VKLObject object);
+OPENVKL_CUDA_INTERFACE void vklRelease(VKLObject object);
+OPENVKL_CUDA_INTERFACE void vklReleaseDevice(VKLDevice);
+
+// ---------------------------------------------------------------------------
+// Data (openvkl/include/openvkl/data.h:38-44).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE VKLData vklNewData(VKLDevice device,
+                                          size_t numItems,
+                                          VKLDataType dataType,
+                                          const void *source,
+                                          VKLDataCreationFlags dataCreationFlags,
+                                          size_t byteStride);
+
+// ---------------------------------------------------------------------------
+// Volumes and parameters (openvkl/include/openvkl/volume.h:53-63,
+// parameters.h:12-32).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE VKLVolume vklNewVolume(VKLDevice device, const char *type);
+OPENVKL_CUDA_INTERFACE vkl_box3f vklGetBoundingBox(VKLVolume volume);
+OPENVKL_CUDA_INTERFACE unsigned int vklGetNumAttributes(VKLVolume volume);
+OPENVKL_CUDA_INTERFACE vkl_range1f vklGetValueRange(VKLVolume volume, unsigned int attributeIndex);
+
+OPENVKL_CUDA_INTERFACE void vklSetBool(VKLObject object, const char *name, int b);
+OPENVKL_CUDA_INTERFACE void vklSetFloat(VKLObject object, const char *name, float x);
+OPENVKL_CUDA_INTERFACE void vklSetVec3f(VKLObject object, const char *name, float x, float y, float z);
+OPENVKL_CUDA_INTERFACE void vklSetInt(VKLObject object, const char *name, int x);
+OPENVKL_CUDA_INTERFACE void vklSetVec3i(VKLObject object, const char *name, int x, int y, int z);
+OPENVKL_CUDA_INTERFACE void vklSetData(VKLObject object, const char *name, VKLData data);
+OPENVKL_CUDA_INTERFACE void vklSetString(VKLObject object, const char *name, const char *s);
+OPENVKL_CUDA_INTERFACE void vklSetVoidPtr(VKLObject object, const char *name, void *v);
+OPENVKL_CUDA_INTERFACE void vklSetParam(VKLObject object, const char *name, VKLDataType dataType,
+                                        const void *mem);
+
+// ---------------------------------------------------------------------------
+// Samplers (openvkl/include/openvkl/sampler.h:30-41).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE VKLSampler vklNewSampler(VKLVolume volume);
+OPENVKL_CUDA_INTERFACE VKLFeatureFlags vklGetFeatureFlags(VKLSampler sampler);
+
+// ---------------------------------------------------------------------------
+// Sampling and gradients
+// (openvkl/devices/cpu/include/openvkl/device/openvkl.h:32-160).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE float vklComputeSample(const VKLSampler *sampler,
+                                              const vkl_vec3f *objectCoordinates,
+                                              unsigned int attributeIndex,
+                                              float time);
+OPENVKL_CUDA_INTERFACE void vklComputeSample4(const int *valid, const VKLSampler *sampler,
+                                              const vkl_vvec3f4 *objectCoordinates,
+                                              float *samples, unsigned int attributeIndex,
+                                              const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSample8(const int *valid, const VKLSampler *sampler,
+                                              const vkl_vvec3f8 *objectCoordinates,
+                                              float *samples, unsigned int attributeIndex,
+                                              const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSample16(const int *valid, const VKLSampler *sampler,
+                                               const vkl_vvec3f16 *objectCoordinates,
+                                               float *samples, unsigned int attributeIndex,
+                                               const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSampleN(const VKLSampler *sampler,
+                                              unsigned int N,
+                                              const vkl_vec3f *objectCoordinates,
+                                              float *samples,
+                                              unsigned int attributeIndex,
+                                              const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSampleM(const VKLSampler *sampler,
+                                              const vkl_vec3f *objectCoordinates,
+                                              float *samples,
+                                              unsigned int M,
+                                              const unsigned int *attributeIndices,
+                                              float time);
+OPENVKL_CUDA_INTERFACE void vklComputeSampleMN(const VKLSampler *sampler,
+                                               unsigned int N,
+                                               const vkl_vec3f *objectCoordinates,
+                                               float *samples,
+                                               unsigned int M,
+                                               const unsigned int *attributeIndices,
+                                               const float *times);
+OPENVKL_CUDA_INTERFACE vkl_vec3f vklComputeGradient(const VKLSampler *sampler,
+                                                    const vkl_vec3f *objectCoordinates,
+                                                    unsigned int attributeIndex,
+                                                    float time);
+OPENVKL_CUDA_INTERFACE void vklComputeGradientN(const VKLSampler *sampler,
+                                                unsigned int N,
+                                                const vkl_vec3f *objectCoordinates,
+                                                vkl_vec3f *gradients,
+                                                unsigned int attributeIndex,
+                                                const float *times);
+
+// ---------------------------------------------------------------------------
+// Iterator contexts (openvkl/include/openvkl/iterator.h:30-37) and the
+// per-ray iterator calls (devices/cpu/include/openvkl/device/openvkl.h:
+// 208-279, :348-416).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE VKLIntervalIteratorContext vklNewIntervalIteratorContext(VKLSampler sampler);
+OPENVKL_CUDA_INTERFACE VKLHitIteratorContext vklNewHitIteratorContext(VKLSampler sampler);
+OPENVKL_CUDA_INTERFACE size_t vklGetIntervalIteratorSize(const VKLIntervalIteratorContext *context);
+OPENVKL_CUDA_INTERFACE VKLIntervalIterator vklInitIntervalIterator(
+    const VKLIntervalIteratorContext *context, const vkl_vec3f *origin,
+    const vkl_vec3f *direction, const vkl_range1f *tRange, float time, void *buffer);
+OPENVKL_CUDA_INTERFACE int vklIterateInterval(VKLIntervalIterator iterator, VKLInterval *interval);
+OPENVKL_CUDA_INTERFACE size_t vklGetHitIteratorSize(const VKLHitIteratorContext *context);
+OPENVKL_CUDA_INTERFACE VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context,
+                                                         const vkl_vec3f *origin,
+                                                         const vkl_vec3f *direction,
+                                                         const vkl_range1f *tRange,
+                                                         float time, void *buffer);
+OPENVKL_CUDA_INTERFACE int vklIterateHit(VKLHitIterator iterator, VKLHit *hit);
+
+// EXTENSION: batched iteration, one GPU thread per ray.  Ray i writes up to
+// `maxPerRay` records at out[i*maxPerRay ...] and its full count to
+// counts[i] (a count above maxPerRay means the ray had more records than
+// were stored).  Records and counts equal what repeated vklIterateInterval /
+// vklIterateHit calls on the same ray return.
+OPENVKL_CUDA_INTERFACE void vklIterateIntervalsN(const VKLIntervalIteratorContext *context,
+                                                 unsigned int N,
+                                                 const vkl_vec3f *origins,
+                                                 const vkl_vec3f *directions,
+                                                 const vkl_range1f *tRanges,
+                                                 unsigned int maxPerRay,
+                                                 VKLInterval *intervals,
+                                                 unsigned int *counts);
+OPENVKL_CUDA_INTERFACE void vklIterateHitsN(const VKLHitIteratorContext *context,
+                                            unsigned int N,
+                                            const vkl_vec3f *origins,
+                                            const vkl_vec3f *directions,
+                                            const vkl_range1f *tRanges,
+                                            unsigned int maxPerRay,
+                                            VKLHit *hits,
+                                            unsigned int *counts);
+
+// ---------------------------------------------------------------------------
+// Observers (openvkl/include/openvkl/observer.h:36-75).
+// ---------------------------------------------------------------------------
+OPENVKL_CUDA_INTERFACE VKLObserver vklNewVolumeObserver(VKLVolume volume, const char *type);
+OPENVKL_CUDA_INTERFACE VKLObserver vklNewSamplerObserver(VKLSampler sampler, const char *type);
+OPENVKL_CUDA_INTERFACE const void *vklMapObserver(VKLObserver observer);
+OPENVKL_CUDA_INTERFACE void vklUnmapObserver(VKLObserver observer);
+OPENVKL_CUDA_INTERFACE VKLDataType vklGetObserverElementType(VKLObserver observer);
+OPENVKL_CUDA_INTERFACE size_t vklGetObserverElementSize(VKLObserver observer);
+OPENVKL_CUDA_INTERFACE size_t vklGetObserverNumElements(VKLObserver observer);
+
+// EXTENSION: copies level `level` (0..2) of a committed volume's tree into
+// host memory: the u64 voxel codes of all nodes (levelNumVoxels per node),
+// their value ranges (2 floats per voxel per attribute) and the node origins
+// (3 u32 per node, relative to the root origin).  Any output may be NULL.
+// Returns the number of nodes on the level (level 3: the number of leaves).
+// Exposes the VdbGrid levels of the reference
+// (openvkl/devices/cpu/volume/vdb/VdbGridShared.h:17-33) for inspection.
+OPENVKL_CUDA_INTERFACE uint64_t vklCudaGetTreeLevel(VKLVolume volume, unsigned int level,
+                                                    uint64_t *voxels, float *valueRanges,
+                                                    uint32_t *origins);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,1009 @@
+// C entry points of the cuda device (include/openvkl_cuda.h).
+//
+// Each call unwraps the {host, device} handle, runs inside a try/catch and
+// converts exceptions into the device's last error plus error callback,
+// returning the reference's sentinel values (NaN sample, null handle, 0)
+// (openvkl/api/API.cpp:37-89, devices/cpu/api/DeviceAPI.cpp:25-57).
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+
+#include "kernels.h"
+#include "objects.h"
+
+using namespace vklcuda;
+
+namespace {
+
+std::mutex g_devicesMutex;
+Device *g_lastDevice = nullptr;
+
+Device *deviceOf(const VKLObject &o)
+{
+  return o.host ? ((ManagedObject *)o.host)->device : g_lastDevice;
+}
+
+template <class F>
+auto guarded(Device *d, F &&f, decltype(f()) onError) -> decltype(f())
+{
+  try {
+    return f();
+  } catch (const VklError &e) {
+    if (d)
+      d->setError(e.code, e.what());
+  } catch (const std::exception &e) {
+    if (d)
+      d->setError(VKL_UNKNOWN_ERROR, e.what());
+  } catch (...) {
+    if (d)
+      d->setError(VKL_UNKNOWN_ERROR, "unknown error");
+  }
+  return onError;
+}
+
+template <class F>
+void guardedVoid(Device *d, F &&f)
+{
+  guarded(
+      d,
+      [&]() {
+        f();
+        return 0;
+      },
+      0);
+}
+
+template <class T>
+T *objectAs(const VKLObject &o, const char *what)
+{
+  T *t = dynamic_cast<T *>((ManagedObject *)o.host);
+  if (!t)
+    fail(std::string("invalid ") + what + " handle", VKL_INVALID_ARGUMENT);
+  return t;
+}
+
+VKLObject handleOf(ManagedObject *o, void *dev = nullptr)
+{
+  VKLObject h;
+  h.host   = o;
+  h.device = dev;
+  return h;
+}
+
+bool isDevicePtr(const void *p)
+{
+  if (!p)
+    return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+const float kNaN = std::numeric_limits<float>::quiet_NaN();
+
+Sampler *committedSampler(const VKLSampler *s)
+{
+  if (!s)
+    fail("sampler is NULL", VKL_INVALID_ARGUMENT);
+  Sampler *sp = objectAs<Sampler>(*s, "sampler");
+  if (!sp->volume || !sp->volume->committed)
+    fail("sampler or its volume is not committed", VKL_INVALID_OPERATION);
+  return sp;
+}
+
+// Runs `launch(devIn, devOut)` on the device stream with inputs / outputs
+// that may be host or device memory; host arrays are staged and the call
+// synchronizes before returning.
+template <class Launch>
+void staged(Device *d, const void *in, size_t inBytes, void *out, size_t outBytes,
+            Launch &&launch)
+{
+  const bool inDev = isDevicePtr(in), outDev = isDevicePtr(out);
+  if (inDev && outDev) {
+    launch(in, out);
+    return;
+  }
+  std::lock_guard<std::mutex> lock(d->stagingMutex);
+  const void *din = in;
+  void *dout      = out;
+  if (!inDev) {
+    d->stageIn.reserve(inBytes);
+    cudaCheck(cudaMemcpyAsync(d->stageIn.ptr, in, inBytes, cudaMemcpyHostToDevice, d->stream),
+              "stage in");
+    din = d->stageIn.ptr;
+  }
+  if (!outDev) {
+    d->stageOut.reserve(outBytes);
+    dout = d->stageOut.ptr;
+  }
+  launch(din, dout);
+  if (!outDev)
+    cudaCheck(cudaMemcpyAsync(out, dout, outBytes, cudaMemcpyDeviceToHost, d->stream),
+              "stage out");
+  cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
+}
+
+void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float *out,
+             uint32_t M, const uint32_t *attrs)
+{
+  Sampler *s = committedSampler(sampler);
+  if (M == 0 || M > kMaxAttributes)
+    fail("invalid number of attributes", VKL_INVALID_ARGUMENT);
+  for (uint32_t m = 0; m < M; ++m)
+    if (attrs[m] >= s->volume->grid.numAttributes)
+      fail("invalid attribute index", VKL_INVALID_ARGUMENT);
+  if (N == 0)
+    return;
+  if (!pts || !out)
+    fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
+  Device *d = s->device;
+  staged(d, pts, N * 12, out, N * 4 * M, [&](const void *din, void *dout) {
+    launchSample(s->volume->grid, s->s.filter, s->s.maxSamplingDepth, N, (const float *)din, M,
+                 attrs, (float *)dout, d->stream);
+  });
+}
+
+void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_vec3f *out,
+               uint32_t attr)
+{
+  Sampler *s = committedSampler(sampler);
+  if (attr >= s->volume->grid.numAttributes)
+    fail("invalid attribute index", VKL_INVALID_ARGUMENT);
+  if (N == 0)
+    return;
+  if (!pts || !out)
+    fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
+  Device *d = s->device;
+  staged(d, pts, N * 12, out, N * 12, [&](const void *din, void *dout) {
+    launchGradient(s->volume->grid, s->s.gradientFilter, s->s.maxSamplingDepth, N,
+                   (const float *)din, attr, (float *)dout, d->stream);
+  });
+}
+
+template <int W, class V>
+void sampleW(const int *valid, const VKLSampler *sampler, const V *oc, float *samples,
+             uint32_t M, const uint32_t *attrs)
+{
+  vkl_vec3f pts[W];
+  int idx[W];
+  int n = 0;
+  for (int i = 0; i < W; ++i)
+    if (!valid || valid[i]) {
+      pts[n] = {oc->x[i], oc->y[i], oc->z[i]};
+      idx[n++] = i;
+    }
+  float out[W * kMaxAttributes];
+  sampleN(sampler, (uint64_t)n, pts, out, M, attrs);
+  for (int k = 0; k < n; ++k)
+    for (uint32_t m = 0; m < M; ++m)
+      samples[m * W + idx[k]] = out[k * M + m];
+}
+
+template <int W, class V>
+void gradientW(const int *valid, const VKLSampler *sampler, const V *oc, V *grads, uint32_t attr)
+{
+  vkl_vec3f pts[W], out[W];
+  int idx[W];
+  int n = 0;
+  for (int i = 0; i < W; ++i)
+    if (!valid || valid[i]) {
+      pts[n] = {oc->x[i], oc->y[i], oc->z[i]};
+      idx[n++] = i;
+    }
+  gradientN(sampler, (uint64_t)n, pts, out, attr);
+  for (int k = 0; k < n; ++k) {
+    grads->x[idx[k]] = out[k].x;
+    grads->y[idx[k]] = out[k].y;
+    grads->z[idx[k]] = out[k].z;
+  }
+}
+
+// Layout of a per-ray iterator inside the caller's buffer.
+constexpr uint32_t kIntervalMagic = 0x564b4c49u;  // "IKLV"
+constexpr uint32_t kHitMagic      = 0x564b4c48u;
+struct IterHeader {
+  uint32_t magic;
+  uint32_t pad;
+  ManagedObject *context;
+};
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// Device.
+// ---------------------------------------------------------------------------
+void vklInit(void) {}
+
+VKLDevice vklNewDevice(const char *name)
+{
+  try {
+    if (!name || (std::strcmp(name, "cuda") != 0 && std::strcmp(name, "cuda_b200") != 0))
+      return nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    Device *d = new Device();
+    cudaGetDevice(&d->cudaDevice);
+    std::lock_guard<std::mutex> lock(g_devicesMutex);
+    g_lastDevice = d;
+    return (VKLDevice)d;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void vklDeviceSetLogCallback(VKLDevice dev, VKLLogCallback cb, void *user)
+{
+  if (!dev)
+    return;
+  ((Device *)dev)->logCb   = cb;
+  ((Device *)dev)->logUser = user;
+}
+
+void vklDeviceSetErrorCallback(VKLDevice dev, VKLErrorCallback cb, void *user)
+{
+  if (!dev)
+    return;
+  ((Device *)dev)->errorCb   = cb;
+  ((Device *)dev)->errorUser = user;
+}
+
+void vklDeviceSetInt(VKLDevice dev, const char *name, int x)
+{
+  if (!dev || !name)
+    return;
+  Device *d = (Device *)dev;
+  d->intParams[name] = x;
+  if (!std::strcmp(name, "logLevel"))
+    d->logLevel = x;
+}
+
+void vklDeviceSetString(VKLDevice dev, const char *name, const char *s)
+{
+  if (!dev || !name)
+    return;
+  ((Device *)dev)->stringParams[name] = s ? s : "";
+}
+
+void vklDeviceSetVoidPtr(VKLDevice dev, const char *name, void *v)
+{
+  if (!dev || !name)
+    return;
+  Device *d = (Device *)dev;
+  if (!std::strcmp(name, "cudaStream"))
+    d->stream = (cudaStream_t)v;
+  else if (!std::strcmp(name, "errorUserData"))
+    d->errorUser = v;
+  else if (!std::strcmp(name, "logUserData"))
+    d->logUser = v;
+}
+
+void vklCommitDevice(VKLDevice dev)
+{
+  if (!dev)
+    return;
+  Device *d = (Device *)dev;
+  guardedVoid(d, [&]() {
+    auto it = d->intParams.find("cudaDevice");
+    if (it != d->intParams.end()) {
+      d->cudaDevice = it->second;
+      cudaCheck(cudaSetDevice(d->cudaDevice), "cudaSetDevice");
+    }
+    d->committed = true;
+  });
+}
+
+VKLError vklDeviceGetLastErrorCode(VKLDevice dev)
+{
+  return dev ? ((Device *)dev)->lastErrorCode : VKL_INVALID_ARGUMENT;
+}
+
+const char *vklDeviceGetLastErrorMsg(VKLDevice dev)
+{
+  return dev ? ((Device *)dev)->lastErrorMsg.c_str() : "invalid device";
+}
+
+int vklGetNativeSIMDWidth(VKLDevice) { return 32; }
+
+void vklCommit(VKLObject object)
+{
+  Device *d = deviceOf(object);
+  guardedVoid(d, [&]() {
+    if (!object.host)
+      fail("vklCommit: NULL handle", VKL_INVALID_ARGUMENT);
+    ManagedObject *o = (ManagedObject *)object.host;
+    o->commit();
+  });
+}
+
+void vklRelease(VKLObject object)
+{
+  Device *d = deviceOf(object);
+  guardedVoid(d, [&]() {
+    if (object.host)
+      ((ManagedObject *)object.host)->refDec();
+  });
+}
+
+void vklReleaseDevice(VKLDevice dev)
+{
+  if (!dev)
+    return;
+  std::lock_guard<std::mutex> lock(g_devicesMutex);
+  if (g_lastDevice == (Device *)dev)
+    g_lastDevice = nullptr;
+  delete (Device *)dev;
+}
+
+// ---------------------------------------------------------------------------
+// Data.
+// ---------------------------------------------------------------------------
+VKLData vklNewData(VKLDevice dev, size_t numItems, VKLDataType type, const void *source,
+                   VKLDataCreationFlags flags, size_t byteStride)
+{
+  Device *d = (Device *)dev;
+  return guarded(
+      d,
+      [&]() -> VKLData {
+        if (!d)
+          fail("vklNewData: NULL device", VKL_INVALID_ARGUMENT);
+        if (numItems && !source)
+          fail("vklNewData: NULL source", VKL_INVALID_ARGUMENT);
+        Data *data     = new Data();
+        data->device   = d;
+        data->type     = type;
+        data->numItems = numItems;
+        if (type & VKL_OBJECT) {
+          const size_t stride = byteStride ? byteStride : sizeof(VKLObject);
+          data->itemSize      = sizeof(VKLObject);
+          for (size_t i = 0; i < numItems; ++i) {
+            const VKLObject *o = (const VKLObject *)((const uint8_t *)source + i * stride);
+            ManagedObject *m   = (ManagedObject *)o->host;
+            if (m)
+              m->refInc();
+            data->objects.push_back(m);
+          }
+          return handleOf(data);
+        }
+        const size_t isz = sizeOfType(type);
+        if (!isz) {
+          delete data;
+          fail("vklNewData: unsupported data type", VKL_INVALID_ARGUMENT);
+        }
+        data->itemSize      = isz;
+        const size_t stride = byteStride ? byteStride : isz;
+        const size_t bytes  = numItems * isz;
+        const bool devSrc   = isDevicePtr(source);
+        if (devSrc && stride == isz && (flags & VKL_DATA_SHARED_BUFFER)) {
+          data->dev = source;  // shared device buffer: used in place
+        } else if (devSrc) {
+          data->owned.alloc(bytes);
+          if (stride == isz)
+            cudaCheck(cudaMemcpyAsync(data->owned.ptr, source, bytes, cudaMemcpyDeviceToDevice,
+                                      d->stream),
+                      "data copy");
+          else
+            cudaCheck(cudaMemcpy2DAsync(data->owned.ptr, isz, source, stride, isz, numItems,
+                                        cudaMemcpyDeviceToDevice, d->stream),
+                      "data copy");
+          cudaCheck(cudaStreamSynchronize(d->stream), "data copy");
+          data->dev = data->owned.ptr;
+        } else {
+          // host source: compact host copy (kept for small arrays) + device copy
+          std::vector<uint8_t> compact(bytes);
+          if (stride == isz)
+            std::memcpy(compact.data(), source, bytes);
+          else
+            for (size_t i = 0; i < numItems; ++i)
+              std::memcpy(&compact[i * isz], (const uint8_t *)source + i * stride, isz);
+          data->owned.alloc(bytes);
+          cudaCheck(cudaMemcpy(data->owned.ptr, compact.data(), bytes, cudaMemcpyHostToDevice),
+                    "data upload");
+          data->dev = data->owned.ptr;
+          if (bytes <= (64u << 20))
+            data->host.swap(compact);
+        }
+        return handleOf(data, (void *)data->dev);
+      },
+      VKLData{nullptr, nullptr});
+}
+
+// ---------------------------------------------------------------------------
+// Volumes and parameters.
+// ---------------------------------------------------------------------------
+VKLVolume vklNewVolume(VKLDevice dev, const char *type)
+{
+  Device *d = (Device *)dev;
+  return guarded(
+      d,
+      [&]() -> VKLVolume {
+        if (!d)
+          fail("vklNewVolume: NULL device", VKL_INVALID_ARGUMENT);
+        const std::string t = type ? type : "";
+        if (t != "structuredRegular" && t != "vdb")
+          fail("unsupported volume type '" + t + "' on the cuda device", VKL_INVALID_ARGUMENT);
+        Volume *v  = new Volume();
+        v->device  = d;
+        v->isDense = (t == "structuredRegular");
+        return handleOf(v);
+      },
+      VKLVolume{nullptr, nullptr});
+}
+
+vkl_box3f vklGetBoundingBox(VKLVolume volume)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> vkl_box3f {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        if (!v->committed)
+          fail("volume is not committed", VKL_INVALID_OPERATION);
+        return v->bounds;
+      },
+      vkl_box3f{{kNaN, kNaN, kNaN}, {kNaN, kNaN, kNaN}});
+}
+
+unsigned int vklGetNumAttributes(VKLVolume volume)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> unsigned int {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        return v->committed ? v->grid.numAttributes : 0u;
+      },
+      0u);
+}
+
+vkl_range1f vklGetValueRange(VKLVolume volume, unsigned int attr)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> vkl_range1f {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        if (!v->committed || attr >= v->grid.numAttributes)
+          fail("invalid attribute index or uncommitted volume", VKL_INVALID_ARGUMENT);
+        return vkl_range1f{v->rangeLo[attr], v->rangeHi[attr]};
+      },
+      vkl_range1f{kNaN, kNaN});
+}
+
+void vklSetParam(VKLObject object, const char *name, VKLDataType type, const void *mem)
+{
+  guardedVoid(deviceOf(object), [&]() {
+    if (!object.host)
+      fail("vklSetParam: NULL handle", VKL_INVALID_ARGUMENT);
+    ((ManagedObject *)object.host)->setParam(name, type, mem);
+  });
+}
+
+void vklSetBool(VKLObject o, const char *name, int b)
+{
+  const int v = b ? 1 : 0;
+  vklSetParam(o, name, VKL_BOOL, &v);
+}
+void vklSetFloat(VKLObject o, const char *name, float x) { vklSetParam(o, name, VKL_FLOAT, &x); }
+void vklSetInt(VKLObject o, const char *name, int x) { vklSetParam(o, name, VKL_INT, &x); }
+void vklSetVec3f(VKLObject o, const char *name, float x, float y, float z)
+{
+  const float v[3] = {x, y, z};
+  vklSetParam(o, name, VKL_VEC3F, v);
+}
+void vklSetVec3i(VKLObject o, const char *name, int x, int y, int z)
+{
+  const int v[3] = {x, y, z};
+  vklSetParam(o, name, VKL_VEC3I, v);
+}
+void vklSetData(VKLObject o, const char *name, VKLData data) { vklSetParam(o, name, VKL_DATA, &data); }
+void vklSetString(VKLObject o, const char *name, const char *s) { vklSetParam(o, name, VKL_STRING, s); }
+void vklSetVoidPtr(VKLObject o, const char *name, void *v) { vklSetParam(o, name, VKL_VOID_PTR, &v); }
+
+// ---------------------------------------------------------------------------
+// Samplers.
+// ---------------------------------------------------------------------------
+VKLSampler vklNewSampler(VKLVolume volume)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> VKLSampler {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        if (!v->committed)
+          fail("vklNewSampler: volume is not committed", VKL_INVALID_OPERATION);
+        Sampler *s = new Sampler();
+        s->device  = v->device;
+        s->volume  = Ref<Volume>(v);
+        s->commit();
+        return handleOf(s, s->devState.ptr);
+      },
+      VKLSampler{nullptr, nullptr});
+}
+
+VKLFeatureFlags vklGetFeatureFlags(VKLSampler sampler)
+{
+  return guarded(
+      deviceOf(sampler),
+      [&]() -> VKLFeatureFlags {
+        Sampler *s = objectAs<Sampler>(sampler, "sampler");
+        VKLFeatureFlags ff = s->volume->isDense ? (1u << 0) : (1u << 5);
+        auto filterBit = [](int f, int base) -> VKLFeatureFlags {
+          return f == VKL_FILTER_NEAREST ? (1u << base)
+                 : f == VKL_FILTER_LINEAR ? (1u << (base + 1))
+                                          : (1u << (base + 2));
+        };
+        ff |= filterBit(s->s.filter, 6) | filterBit(s->s.gradientFilter, 9);
+        ff |= 1u << 12;  // temporally constant
+        ff |= (s->volume->isDense || !s->volume->has("nodesPackedDense")) ? (1u << 20) : (1u << 19);
+        return ff;
+      },
+      (VKLFeatureFlags)0);
+}
+
+// ---------------------------------------------------------------------------
+// Sampling.
+// ---------------------------------------------------------------------------
+float vklComputeSample(const VKLSampler *sampler, const vkl_vec3f *oc, unsigned int attr,
+                       float /*time*/)
+{
+  return guarded(
+      sampler ? deviceOf(*sampler) : g_lastDevice,
+      [&]() -> float {
+        float out = kNaN;
+        sampleN(sampler, 1, oc, &out, 1, &attr);
+        return out;
+      },
+      kNaN);
+}
+
+void vklComputeSample4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc,
+                       float *samples, unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice,
+              [&]() { sampleW<4>(valid, s, oc, samples, 1, &attr); });
+}
+void vklComputeSample8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc,
+                       float *samples, unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice,
+              [&]() { sampleW<8>(valid, s, oc, samples, 1, &attr); });
+}
+void vklComputeSample16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc,
+                        float *samples, unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice,
+              [&]() { sampleW<16>(valid, s, oc, samples, 1, &attr); });
+}
+
+void vklComputeSampleN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
+                       float *samples, unsigned int attr, const float * /*times*/)
+{
+  guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
+              [&]() { sampleN(sampler, N, oc, samples, 1, &attr); });
+}
+
+void vklComputeSampleM(const VKLSampler *sampler, const vkl_vec3f *oc, float *samples,
+                       unsigned int M, const unsigned int *attrs, float /*time*/)
+{
+  guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
+              [&]() { sampleN(sampler, 1, oc, samples, M, attrs); });
+}
+
+void vklComputeSampleMN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
+                        float *samples, unsigned int M, const unsigned int *attrs,
+                        const float * /*times*/)
+{
+  guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
+              [&]() { sampleN(sampler, N, oc, samples, M, attrs); });
+}
+
+vkl_vec3f vklComputeGradient(const VKLSampler *sampler, const vkl_vec3f *oc, unsigned int attr,
+                             float /*time*/)
+{
+  return guarded(
+      sampler ? deviceOf(*sampler) : g_lastDevice,
+      [&]() -> vkl_vec3f {
+        vkl_vec3f g{kNaN, kNaN, kNaN};
+        gradientN(sampler, 1, oc, &g, attr);
+        return g;
+      },
+      vkl_vec3f{kNaN, kNaN, kNaN});
+}
+
+void vklComputeGradientN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
+                         vkl_vec3f *gradients, unsigned int attr, const float * /*times*/)
+{
+  guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
+              [&]() { gradientN(sampler, N, oc, gradients, attr); });
+}
+
+// ---------------------------------------------------------------------------
+// Iterator contexts.
+// ---------------------------------------------------------------------------
+VKLIntervalIteratorContext vklNewIntervalIteratorContext(VKLSampler sampler)
+{
+  return guarded(
+      deviceOf(sampler),
+      [&]() -> VKLIntervalIteratorContext {
+        Sampler *s         = objectAs<Sampler>(sampler, "sampler");
+        IntervalContext *c = new IntervalContext();
+        c->device          = s->device;
+        c->sampler         = Ref<Sampler>(s);
+        c->commit();
+        return handleOf(c);
+      },
+      VKLIntervalIteratorContext{nullptr, nullptr});
+}
+
+VKLHitIteratorContext vklNewHitIteratorContext(VKLSampler sampler)
+{
+  return guarded(
+      deviceOf(sampler),
+      [&]() -> VKLHitIteratorContext {
+        Sampler *s    = objectAs<Sampler>(sampler, "sampler");
+        HitContext *c = new HitContext();
+        c->device     = s->device;
+        c->sampler    = Ref<Sampler>(s);
+        c->commit();
+        return handleOf(c);
+      },
+      VKLHitIteratorContext{nullptr, nullptr});
+}
+
+size_t vklGetIntervalIteratorSize(const VKLIntervalIteratorContext *)
+{
+  return sizeof(IterHeader) + intervalIterStateSize();
+}
+
+size_t vklGetHitIteratorSize(const VKLHitIteratorContext *)
+{
+  return sizeof(IterHeader) + hitIterStateSize();
+}
+
+VKLIntervalIterator vklInitIntervalIterator(const VKLIntervalIteratorContext *context,
+                                            const vkl_vec3f *origin, const vkl_vec3f *direction,
+                                            const vkl_range1f *tRange, float /*time*/,
+                                            void *buffer)
+{
+  return guarded(
+      context ? deviceOf(*context) : g_lastDevice,
+      [&]() -> VKLIntervalIterator {
+        if (!context || !buffer || !origin || !direction || !tRange)
+          fail("vklInitIntervalIterator: NULL argument", VKL_INVALID_ARGUMENT);
+        IntervalContext *c = objectAs<IntervalContext>(*context, "interval iterator context");
+        Device *d          = c->device;
+        IterHeader *h      = (IterHeader *)buffer;
+        h->magic           = kIntervalMagic;
+        h->context         = c;
+        const float ray[8] = {origin->x, origin->y, origin->z, direction->x, direction->y,
+                              direction->z, tRange->lower, tRange->upper};
+        std::lock_guard<std::mutex> lock(d->stagingMutex);
+        const size_t ss = intervalIterStateSize();
+        d->stageAux.reserve(ss + 64);
+        cudaCheck(cudaMemcpyAsync(d->stageAux.as<uint8_t>() + ss, ray, sizeof(ray),
+                                  cudaMemcpyHostToDevice, d->stream),
+                  "iterator init");
+        launchIntervalIterInit(c->sampler->volume->grid, c->attr, c->depth,
+                               (const float *)(d->stageAux.as<uint8_t>() + ss), d->stageAux.ptr,
+                               d->stream);
+        cudaCheck(cudaMemcpyAsync(h + 1, d->stageAux.ptr, ss, cudaMemcpyDeviceToHost, d->stream),
+                  "iterator init");
+        cudaCheck(cudaStreamSynchronize(d->stream), "iterator init");
+        return (VKLIntervalIterator)buffer;
+      },
+      (VKLIntervalIterator) nullptr);
+}
+
+int vklIterateInterval(VKLIntervalIterator iterator, VKLInterval *interval)
+{
+  IterHeader *h = (IterHeader *)iterator;
+  Device *d     = (h && h->magic == kIntervalMagic) ? h->context->device : g_lastDevice;
+  return guarded(
+      d,
+      [&]() -> int {
+        if (!h || h->magic != kIntervalMagic || !interval)
+          fail("vklIterateInterval: invalid iterator", VKL_INVALID_ARGUMENT);
+        IntervalContext *c = (IntervalContext *)h->context;
+        std::lock_guard<std::mutex> lock(d->stagingMutex);
+        const size_t ss = intervalIterStateSize();
+        d->stageAux.reserve(ss + 64);
+        uint8_t *base = d->stageAux.as<uint8_t>();
+        cudaCheck(cudaMemcpyAsync(base, h + 1, ss, cudaMemcpyHostToDevice, d->stream), "iterate");
+        DevInterval *dOut = (DevInterval *)(base + ((ss + 15) & ~size_t(15)));
+        int *dRes         = (int *)(dOut + 1);
+        launchIntervalIterNext(c->sampler->volume->grid, c->devValueRanges(), base, dOut, dRes,
+                               d->stream);
+        struct {
+          DevInterval iv;
+          int res;
+        } out;
+        cudaCheck(cudaMemcpyAsync(h + 1, base, ss, cudaMemcpyDeviceToHost, d->stream), "iterate");
+        cudaCheck(cudaMemcpyAsync(&out, dOut, sizeof(out), cudaMemcpyDeviceToHost, d->stream),
+                  "iterate");
+        cudaCheck(cudaStreamSynchronize(d->stream), "iterate");
+        if (out.res) {
+          interval->tRange        = {out.iv.t0, out.iv.t1};
+          interval->valueRange    = {out.iv.v0, out.iv.v1};
+          interval->nominalDeltaT = out.iv.nominalDeltaT;
+        }
+        return out.res;
+      },
+      0);
+}
+
+VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context, const vkl_vec3f *origin,
+                                  const vkl_vec3f *direction, const vkl_range1f *tRange,
+                                  float /*time*/, void *buffer)
+{
+  return guarded(
+      context ? deviceOf(*context) : g_lastDevice,
+      [&]() -> VKLHitIterator {
+        if (!context || !buffer || !origin || !direction || !tRange)
+          fail("vklInitHitIterator: NULL argument", VKL_INVALID_ARGUMENT);
+        HitContext *c      = objectAs<HitContext>(*context, "hit iterator context");
+        Device *d          = c->device;
+        IterHeader *h      = (IterHeader *)buffer;
+        h->magic           = kHitMagic;
+        h->context         = c;
+        const float ray[8] = {origin->x, origin->y, origin->z, direction->x, direction->y,
+                              direction->z, tRange->lower, tRange->upper};
+        std::lock_guard<std::mutex> lock(d->stagingMutex);
+        const size_t ss = hitIterStateSize();
+        d->stageAux.reserve(ss + 64);
+        cudaCheck(cudaMemcpyAsync(d->stageAux.as<uint8_t>() + ss, ray, sizeof(ray),
+                                  cudaMemcpyHostToDevice, d->stream),
+                  "iterator init");
+        launchHitIterInit(c->sampler->volume->grid, c->attr, c->depth,
+                          (const float *)(d->stageAux.as<uint8_t>() + ss), d->stageAux.ptr,
+                          d->stream);
+        cudaCheck(cudaMemcpyAsync(h + 1, d->stageAux.ptr, ss, cudaMemcpyDeviceToHost, d->stream),
+                  "iterator init");
+        cudaCheck(cudaStreamSynchronize(d->stream), "iterator init");
+        return (VKLHitIterator)buffer;
+      },
+      (VKLHitIterator) nullptr);
+}
+
+int vklIterateHit(VKLHitIterator iterator, VKLHit *hit)
+{
+  IterHeader *h = (IterHeader *)iterator;
+  Device *d     = (h && h->magic == kHitMagic) ? h->context->device : g_lastDevice;
+  return guarded(
+      d,
+      [&]() -> int {
+        if (!h || h->magic != kHitMagic || !hit)
+          fail("vklIterateHit: invalid iterator", VKL_INVALID_ARGUMENT);
+        HitContext *c = (HitContext *)h->context;
+        std::lock_guard<std::mutex> lock(d->stagingMutex);
+        const size_t ss = hitIterStateSize();
+        d->stageAux.reserve(ss + 64);
+        uint8_t *base = d->stageAux.as<uint8_t>();
+        cudaCheck(cudaMemcpyAsync(base, h + 1, ss, cudaMemcpyHostToDevice, d->stream), "iterate");
+        DevHit *dOut = (DevHit *)(base + ((ss + 15) & ~size_t(15)));
+        int *dRes    = (int *)(dOut + 1);
+        launchHitIterNext(c->sampler->volume->grid, c->sampler->s.filter, c->devValueRanges(),
+                          (uint32_t)c->values.size(), c->devValues.as<float>(), base, dOut, dRes,
+                          d->stream);
+        struct {
+          DevHit hit;
+          int res;
+        } out;
+        cudaCheck(cudaMemcpyAsync(h + 1, base, ss, cudaMemcpyDeviceToHost, d->stream), "iterate");
+        cudaCheck(cudaMemcpyAsync(&out, dOut, sizeof(out), cudaMemcpyDeviceToHost, d->stream),
+                  "iterate");
+        cudaCheck(cudaStreamSynchronize(d->stream), "iterate");
+        if (out.res) {
+          hit->t       = out.hit.t;
+          hit->sample  = out.hit.sample;
+          hit->epsilon = out.hit.epsilon;
+        }
+        return out.res;
+      },
+      0);
+}
+
+void vklIterateIntervalsN(const VKLIntervalIteratorContext *context, unsigned int N,
+                          const vkl_vec3f *origins, const vkl_vec3f *directions,
+                          const vkl_range1f *tRanges, unsigned int maxPerRay,
+                          VKLInterval *intervals, unsigned int *counts)
+{
+  guardedVoid(context ? deviceOf(*context) : g_lastDevice, [&]() {
+    if (!context)
+      fail("NULL context", VKL_INVALID_ARGUMENT);
+    IntervalContext *c = objectAs<IntervalContext>(*context, "interval iterator context");
+    Device *d          = c->device;
+    if (!N)
+      return;
+    const bool dev = isDevicePtr(origins) && isDevicePtr(directions) && isDevicePtr(tRanges) &&
+                     isDevicePtr(counts) && (maxPerRay == 0 || isDevicePtr(intervals));
+    const DevGrid &g = c->sampler->volume->grid;
+    if (dev) {
+      launchIntervals(g, c->attr, c->depth, c->devValueRanges(), N, (const float *)origins,
+                      (const float *)directions, (const float *)tRanges, maxPerRay,
+                      (DevInterval *)intervals, counts, d->stream);
+      return;
+    }
+    std::lock_guard<std::mutex> lock(d->stagingMutex);
+    const size_t inB = (size_t)N * 32, outB = (size_t)N * maxPerRay * 20 + (size_t)N * 4;
+    d->stageIn.reserve(inB);
+    d->stageOut.reserve(outB);
+    uint8_t *in = d->stageIn.as<uint8_t>(), *out = d->stageOut.as<uint8_t>();
+    cudaCheck(cudaMemcpyAsync(in, origins, N * 12, cudaMemcpyHostToDevice, d->stream), "stage");
+    cudaCheck(cudaMemcpyAsync(in + N * 12, directions, N * 12, cudaMemcpyHostToDevice, d->stream),
+              "stage");
+    cudaCheck(cudaMemcpyAsync(in + N * 24, tRanges, N * 8, cudaMemcpyHostToDevice, d->stream),
+              "stage");
+    DevInterval *dIv = (DevInterval *)out;
+    uint32_t *dCnt   = (uint32_t *)(out + (size_t)N * maxPerRay * 20);
+    launchIntervals(g, c->attr, c->depth, c->devValueRanges(), N, (const float *)in,
+                    (const float *)(in + N * 12), (const float *)(in + N * 24), maxPerRay, dIv,
+                    dCnt, d->stream);
+    if (maxPerRay)
+      cudaCheck(cudaMemcpyAsync(intervals, dIv, (size_t)N * maxPerRay * 20, cudaMemcpyDeviceToHost,
+                                d->stream),
+                "stage");
+    cudaCheck(cudaMemcpyAsync(counts, dCnt, (size_t)N * 4, cudaMemcpyDeviceToHost, d->stream),
+              "stage");
+    cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
+  });
+}
+
+void vklIterateHitsN(const VKLHitIteratorContext *context, unsigned int N,
+                     const vkl_vec3f *origins, const vkl_vec3f *directions,
+                     const vkl_range1f *tRanges, unsigned int maxPerRay, VKLHit *hits,
+                     unsigned int *counts)
+{
+  guardedVoid(context ? deviceOf(*context) : g_lastDevice, [&]() {
+    if (!context)
+      fail("NULL context", VKL_INVALID_ARGUMENT);
+    HitContext *c = objectAs<HitContext>(*context, "hit iterator context");
+    Device *d     = c->device;
+    if (!N)
+      return;
+    const bool dev = isDevicePtr(origins) && isDevicePtr(directions) && isDevicePtr(tRanges) &&
+                     isDevicePtr(counts) && (maxPerRay == 0 || isDevicePtr(hits));
+    const DevGrid &g = c->sampler->volume->grid;
+    const int filter = c->sampler->s.filter;
+    if (dev) {
+      launchHits(g, c->attr, filter, c->depth, c->devValueRanges(), (uint32_t)c->values.size(),
+                 c->devValues.as<float>(), N, (const float *)origins, (const float *)directions,
+                 (const float *)tRanges, maxPerRay, (DevHit *)hits, counts, d->stream);
+      return;
+    }
+    std::lock_guard<std::mutex> lock(d->stagingMutex);
+    const size_t inB = (size_t)N * 32, outB = (size_t)N * maxPerRay * 12 + (size_t)N * 4;
+    d->stageIn.reserve(inB);
+    d->stageOut.reserve(outB);
+    uint8_t *in = d->stageIn.as<uint8_t>(), *out = d->stageOut.as<uint8_t>();
+    cudaCheck(cudaMemcpyAsync(in, origins, N * 12, cudaMemcpyHostToDevice, d->stream), "stage");
+    cudaCheck(cudaMemcpyAsync(in + N * 12, directions, N * 12, cudaMemcpyHostToDevice, d->stream),
+              "stage");
+    cudaCheck(cudaMemcpyAsync(in + N * 24, tRanges, N * 8, cudaMemcpyHostToDevice, d->stream),
+              "stage");
+    DevHit *dHit   = (DevHit *)out;
+    uint32_t *dCnt = (uint32_t *)(out + (size_t)N * maxPerRay * 12);
+    launchHits(g, c->attr, filter, c->depth, c->devValueRanges(), (uint32_t)c->values.size(),
+               c->devValues.as<float>(), N, (const float *)in, (const float *)(in + N * 12),
+               (const float *)(in + N * 24), maxPerRay, dHit, dCnt, d->stream);
+    if (maxPerRay)
+      cudaCheck(cudaMemcpyAsync(hits, dHit, (size_t)N * maxPerRay * 12, cudaMemcpyDeviceToHost,
+                                d->stream),
+                "stage");
+    cudaCheck(cudaMemcpyAsync(counts, dCnt, (size_t)N * 4, cudaMemcpyDeviceToHost, d->stream),
+              "stage");
+    cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Observers.
+// ---------------------------------------------------------------------------
+VKLObserver vklNewVolumeObserver(VKLVolume volume, const char *type)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> VKLObserver {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        if (!v->committed)
+          fail("Trying to create an observer on a vdb volume that was not committed.",
+               VKL_INVALID_OPERATION);
+        const std::string t = type ? type : "";
+        if (t != "InnerNode")
+          fail("unsupported volume observer type '" + t + "'", VKL_INVALID_ARGUMENT);
+        Observer *o = new Observer();
+        o->device   = v->device;
+        o->volume   = Ref<Volume>(v);
+        o->kind     = t;
+        return handleOf(o);
+      },
+      VKLObserver{nullptr, nullptr});
+}
+
+VKLObserver vklNewSamplerObserver(VKLSampler sampler, const char *type)
+{
+  return guarded(
+      deviceOf(sampler),
+      [&]() -> VKLObserver {
+        objectAs<Sampler>(sampler, "sampler");
+        fail(std::string("unsupported sampler observer type '") + (type ? type : "") + "'",
+             VKL_INVALID_ARGUMENT);
+      },
+      VKLObserver{nullptr, nullptr});
+}
+
+const void *vklMapObserver(VKLObserver observer)
+{
+  return guarded(
+      deviceOf(observer),
+      [&]() -> const void * {
+        Observer *o = objectAs<Observer>(observer, "observer");
+        o->commit();
+        return o->buffer.data();
+      },
+      (const void *)nullptr);
+}
+
+void vklUnmapObserver(VKLObserver) {}
+
+VKLDataType vklGetObserverElementType(VKLObserver observer)
+{
+  return guarded(
+      deviceOf(observer),
+      [&]() -> VKLDataType {
+        objectAs<Observer>(observer, "observer");
+        return VKL_OBJECT;
+      },
+      VKL_UNKNOWN);
+}
+
+size_t vklGetObserverElementSize(VKLObserver observer)
+{
+  return guarded(
+      deviceOf(observer),
+      [&]() -> size_t { return objectAs<Observer>(observer, "observer")->elementFloats * 4; },
+      (size_t)0);
+}
+
+size_t vklGetObserverNumElements(VKLObserver observer)
+{
+  return guarded(
+      deviceOf(observer),
+      [&]() -> size_t { return objectAs<Observer>(observer, "observer")->numElements; },
+      (size_t)0);
+}
+
+uint64_t vklCudaGetTreeLevel(VKLVolume volume, unsigned int level, uint64_t *voxels,
+                             float *valueRanges, uint32_t *origins)
+{
+  return guarded(
+      deviceOf(volume),
+      [&]() -> uint64_t {
+        Volume *v = objectAs<Volume>(volume, "volume");
+        if (!v->committed)
+          fail("volume is not committed", VKL_INVALID_OPERATION);
+        if (level >= kNumLevels)
+          fail("invalid level", VKL_INVALID_ARGUMENT);
+        if (level == kNumLevels - 1)
+          return v->grid.numLeaves;
+        const DevLevel &L = v->grid.levels[level];
+        const uint64_t nv = L.numNodes * levelNumVoxels(level);
+        if (voxels)
+          cudaCheck(cudaMemcpy(voxels, L.voxels, nv * 8, cudaMemcpyDeviceToHost), "readback");
+        if (valueRanges)
+          cudaCheck(cudaMemcpy(valueRanges, L.valueRange, nv * 8 * v->grid.numAttributes,
+                               cudaMemcpyDeviceToHost),
+                    "readback");
+        if (origins)
+          cudaCheck(cudaMemcpy(origins, L.origin, L.numNodes * 12, cudaMemcpyDeviceToHost),
+                    "readback");
+        return L.numNodes;
+      },
+      (uint64_t)0);
+}
+
+}  // extern "C"

@@ -1,0 +1,375 @@
+// Commit-time kernels of the cuda device: dense tree construction and the
+// value-range builder (per-leaf filter-support ranges, then propagation up
+// the tree), the reference's VdbVolume::commit hot loops
+// (openvkl/devices/cpu/volume/vdb/VdbVolume.cpp:338-392,
+// VdbSampler.ispc:383-557) as GPU kernels.
+#include "kernels.h"
+#include "objects.h"
+#include "sampling.cuh"
+
+namespace vklcuda {
+
+namespace {
+
+constexpr float kInf = __builtin_huge_valf();
+
+__device__ __forceinline__ float fminx(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmaxx(float a, float b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Dense tree.  Leaves are inserted in x-fastest order, so level-l nodes are
+// numbered in (z, y, x)-lexicographic order of their origins, which is what
+// the reference's first-come insertion (VdbVolume.cpp:244-331) produces.
+// ---------------------------------------------------------------------------
+__global__ void kDenseLevel2(uint64_t *vox2, uint32_t *org2, uint3 nl, uint3 n2)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t total = (uint64_t)n2.x * n2.y * n2.z * 4096;
+  if (i >= total)
+    return;
+  const uint64_t k2 = i >> 12;
+  const uint32_t v  = (uint32_t)(i & 4095);
+  const uint32_t vx = v >> 8, vy = (v >> 4) & 15, vz = v & 15;
+  const uint32_t x2 = (uint32_t)(k2 % n2.x), y2 = (uint32_t)((k2 / n2.x) % n2.y),
+                 z2 = (uint32_t)(k2 / ((uint64_t)n2.x * n2.y));
+  const uint32_t lx = x2 * 16 + vx, ly = y2 * 16 + vy, lz = z2 * 16 + vz;
+  uint64_t code = 0;
+  if (lx < nl.x && ly < nl.y && lz < nl.z)
+    code = voxelMakeLeaf(((uint64_t)lz * nl.y + ly) * nl.x + lx, kFormatDenseZYX, 0);
+  vox2[i] = code;
+  if (v == 0) {
+    org2[3 * k2]     = x2 * 128;
+    org2[3 * k2 + 1] = y2 * 128;
+    org2[3 * k2 + 2] = z2 * 128;
+  }
+}
+
+__global__ void kDenseLevel1(uint64_t *vox1, uint32_t *org1, uint3 n2, uint3 n1)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t total = (uint64_t)n1.x * n1.y * n1.z * 32768;
+  if (i >= total)
+    return;
+  const uint64_t k1 = i >> 15;
+  const uint32_t v  = (uint32_t)(i & 32767);
+  const uint32_t vx = v >> 10, vy = (v >> 5) & 31, vz = v & 31;
+  const uint32_t x1 = (uint32_t)(k1 % n1.x), y1 = (uint32_t)((k1 / n1.x) % n1.y),
+                 z1 = (uint32_t)(k1 / ((uint64_t)n1.x * n1.y));
+  const uint32_t x2 = x1 * 32 + vx, y2 = y1 * 32 + vy, z2 = z1 * 32 + vz;
+  uint64_t code = 0;
+  if (x2 < n2.x && y2 < n2.y && z2 < n2.z)
+    code = voxelMakeChild(((uint64_t)z2 * n2.y + y2) * n2.x + x2);
+  vox1[i] = code;
+  if (v == 0) {
+    org1[3 * k1]     = x1 * 4096;
+    org1[3 * k1 + 1] = y1 * 4096;
+    org1[3 * k1 + 2] = z1 * 4096;
+  }
+}
+
+__global__ void kDenseLevel0(uint64_t *vox0, uint3 n1)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 262144)
+    return;
+  const uint32_t vx = i >> 12, vy = (i >> 6) & 63, vz = i & 63;
+  uint64_t code = 0;
+  if (vx < n1.x && vy < n1.y && vz < n1.z)
+    code = voxelMakeChild(((uint64_t)vz * n1.y + vy) * n1.x + vx);
+  vox0[i] = code;
+}
+
+// ---------------------------------------------------------------------------
+// Dense leaf ranges.  The reference scans, for each leaf, the voxel windows
+// [7,8) | [0,8) | [0,2) of its 3x3x3 leaf neighbourhood, skipping voxels
+// outside the dense dimensions, and adds the background for neighbours whose
+// origin lies outside the domain (VdbSampler.ispc:460-557,
+// VdbSampler_dense.ih:35-105).  Per axis that is the clipped voxel box
+// [o-1, o+10); the background joins when o-8 < 0 or o+8 >= dims on any axis
+// and is skipped when NaN.  min/max are exact, so the scan order is free.
+//
+// One thread per (leaf, x-window column): a block covers 32 consecutive
+// leaves along x for one (ly, lz), so a warp's loads along a row are
+// contiguous; the 11x11 (y,z) rows of the window are read through L1/L2.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) kDenseLeafRanges(const __grid_constant__ DevGrid g,
+                                                        uint32_t attr, uint3 nl,
+                                                        float *__restrict__ leafRanges)
+{
+  const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t numLeaves = (uint64_t)nl.x * nl.y * nl.z;
+  if (leaf >= numLeaves)
+    return;
+  const uint32_t lx = (uint32_t)(leaf % nl.x), ly = (uint32_t)((leaf / nl.x) % nl.y),
+                 lz = (uint32_t)(leaf / ((uint64_t)nl.x * nl.y));
+  const int32_t X = g.denseDims[0], Y = g.denseDims[1], Z = g.denseDims[2];
+  const int32_t ox = (int32_t)lx * 8, oy = (int32_t)ly * 8, oz = (int32_t)lz * 8;
+  const int32_t x0 = max(ox - 1, 0), x1 = min(ox + 10, X);
+  const int32_t y0 = max(oy - 1, 0), y1 = min(oy + 10, Y);
+  const int32_t z0 = max(oz - 1, 0), z1 = min(oz + 10, Z);
+  const T *data = (const T *)g.data[attr];
+  float lo = kInf, hi = -kInf;
+  for (int32_t z = z0; z < z1; ++z)
+    for (int32_t y = y0; y < y1; ++y) {
+      const T *row = data + ((uint64_t)z * Y + y) * (uint64_t)X;
+      for (int32_t x = x0; x < x1; ++x) {
+        const float v = ldv(row, x);
+        lo            = fminx(lo, v);
+        hi            = fmaxx(hi, v);
+      }
+    }
+  const bool boundary = ox - 8 < 0 || oy - 8 < 0 || oz - 8 < 0 || ox + 8 >= X || oy + 8 >= Y ||
+                        oz + 8 >= Z;
+  const float bg = g.background[attr];
+  if (boundary && !isnan(bg)) {
+    lo = fminx(lo, bg);
+    hi = fmaxx(hi, bg);
+  }
+  leafRanges[2 * leaf]     = lo;
+  leafRanges[2 * leaf + 1] = hi;
+}
+
+// ---------------------------------------------------------------------------
+// Sparse leaf ranges: per leaf, walk to each of the 27 neighbour leaves and
+// scan its window (VdbSampler_computeNodeValueRange, VdbSampler.ispc:
+// 383-455; packed handlers VdbSampler_packed_denseZYX.ih:12-75,
+// VdbSampler_packed_tile.ih).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) kSparseLeafRanges(const __grid_constant__ DevGrid g,
+                                                         uint32_t attr, uint64_t numLeaves,
+                                                         const uint32_t *__restrict__ offs,
+                                                         float *__restrict__ leafRanges)
+{
+  const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= numLeaves)
+    return;
+  const SparseField<T> F(g, attr, kNumLevels - 1);
+  const uint32_t cx = offs[3 * leaf], cy = offs[3 * leaf + 1], cz = offs[3 * leaf + 2];
+  const float bgOut = g.background[attr];
+  float lo = kInf, hi = -kInf;
+  for (int n = 0; n < 27; ++n) {
+    const int ix = n / 9, iy = (n / 3) % 3, iz = n % 3;
+    const uint32_t dx = cx + (uint32_t)((ix - 1) * 8), dy = cy + (uint32_t)((iy - 1) * 8),
+                   dz = cz + (uint32_t)((iz - 1) * 8);
+    float nlo, nhi;
+    const bool inDom = F.inDomain(dx, dy, dz);
+    const uint64_t voxel = inDom ? F.traverse(dx, dy, dz) : 0ull;
+    if (!voxelIsLeaf(voxel)) {
+      nlo = nhi = inDom ? 0.f : bgOut;
+    } else if (voxelLeafFormat(voxel) == kFormatTile) {
+      nlo = nhi = ldv((const T *)g.tile[attr], voxelLeafIndex(voxel));
+    } else {
+      const uint32_t xa = ix == 0 ? 7 : 0, xb = ix == 2 ? 2 : 8;
+      const uint32_t ya = iy == 0 ? 7 : 0, yb = iy == 2 ? 2 : 8;
+      const uint32_t za = iz == 0 ? 7 : 0, zb = iz == 2 ? 2 : 8;
+      const T *base = (const T *)g.data[attr] + voxelLeafIndex(voxel) * 512;
+      nlo = kInf;
+      nhi = -kInf;
+      for (uint32_t x = xa; x < xb; ++x)
+        for (uint32_t y = ya; y < yb; ++y)
+          for (uint32_t z = za; z < zb; ++z) {
+            const float v = ldv(base, (x << 6) + (y << 3) + z);
+            nlo           = fminx(nlo, v);
+            nhi           = fmaxx(nhi, v);
+          }
+    }
+    if (!isnan(nlo))
+      lo = fminx(lo, nlo);
+    if (!isnan(nhi))
+      hi = fmaxx(hi, nhi);
+  }
+  leafRanges[2 * leaf]     = lo;
+  leafRanges[2 * leaf + 1] = hi;
+}
+
+// ---------------------------------------------------------------------------
+// Propagation.  Every leaf's range lands in the voxel that points at it;
+// every child node's voxels reduce into the voxel that points at the node.
+// This equals the reference's per-leaf `extend` up the ancestor chain
+// (VdbVolume.cpp:361-391) because min/max are order-independent.
+// ---------------------------------------------------------------------------
+__global__ void kFillEmpty(float *r, uint64_t n)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    r[2 * i]     = kInf;
+    r[2 * i + 1] = -kInf;
+  }
+}
+
+__global__ void kLeafToParent(const __grid_constant__ DevGrid g, uint32_t attr, uint64_t numLeaves,
+                              const uint64_t *__restrict__ leafVoxel,
+                              const float *__restrict__ leafRanges, uint3 nl)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= numLeaves)
+    return;
+  uint64_t lv;
+  if (leafVoxel) {
+    lv = leafVoxel[i];
+    if (lv == ~0ull)
+      return;
+  } else {
+    // dense: leaf (lx,ly,lz) hangs off level-2 node (l>>4) at voxel (l&15)
+    const uint32_t lx = (uint32_t)(i % nl.x), ly = (uint32_t)((i / nl.x) % nl.y),
+                   lz = (uint32_t)(i / ((uint64_t)nl.x * nl.y));
+    const uint32_t n2x = (nl.x + 15) / 16, n2y = (nl.y + 15) / 16;
+    const uint64_t k2 = ((uint64_t)(lz >> 4) * n2y + (ly >> 4)) * n2x + (lx >> 4);
+    lv = (2ull << 40) | (k2 * 4096 + ((lx & 15) << 8) + ((ly & 15) << 4) + (lz & 15));
+  }
+  const uint32_t level = (uint32_t)(lv >> 40);
+  const uint64_t v     = lv & ((1ull << 40) - 1);
+  float *r = (float *)g.levels[level].valueRange + 2 * (v * g.numAttributes + attr);
+  // A voxel holds exactly one leaf, so this read-modify-write has no race;
+  // it extends like the reference instead of assigning.
+  r[0] = fminx(r[0], leafRanges[2 * i]);
+  r[1] = fmaxx(r[1], leafRanges[2 * i + 1]);
+}
+
+// One block per node on `level` (1 or 2): reduce the node's voxel ranges and
+// write them into the parent voxel on level-1, found by walking down from
+// the root with the node's origin.
+__global__ void __launch_bounds__(256) kReduceNodes(const __grid_constant__ DevGrid g,
+                                                    uint32_t attr, uint32_t level)
+{
+  const uint64_t node = blockIdx.x;
+  const DevLevel &L   = g.levels[level];
+  const uint64_t nv   = levelNumVoxels(level);
+  float lo = kInf, hi = -kInf;
+  for (uint64_t v = threadIdx.x; v < nv; v += blockDim.x) {
+    const float *r = L.valueRange + 2 * ((node * nv + v) * g.numAttributes + attr);
+    lo             = fminx(lo, r[0]);
+    hi             = fmaxx(hi, r[1]);
+  }
+  __shared__ float slo[256], shi[256];
+  slo[threadIdx.x] = lo;
+  shi[threadIdx.x] = hi;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      slo[threadIdx.x] = fminx(slo[threadIdx.x], slo[threadIdx.x + s]);
+      shi[threadIdx.x] = fmaxx(shi[threadIdx.x], shi[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const uint32_t ox = L.origin[3 * node], oy = L.origin[3 * node + 1], oz = L.origin[3 * node + 2];
+    uint64_t pnode = 0;
+    for (uint32_t l = 0; l + 1 < level; ++l) {
+      const uint64_t v = g.levels[l].voxels[pnode * levelNumVoxels(l) + offsetToLinear(l, ox, oy, oz)];
+      pnode            = voxelChildIndex(v);
+    }
+    const uint32_t pl = level - 1;
+    const uint64_t pv = pnode * levelNumVoxels(pl) + offsetToLinear(pl, ox, oy, oz);
+    float *r = (float *)g.levels[pl].valueRange + 2 * (pv * g.numAttributes + attr);
+    r[0]     = fminx(r[0], slo[0]);
+    r[1]     = fmaxx(r[1], shi[0]);
+  }
+}
+
+__global__ void __launch_bounds__(1024) kVolumeRange(const __grid_constant__ DevGrid g,
+                                                     uint32_t attr, float *out)
+{
+  float lo = kInf, hi = -kInf;
+  for (uint32_t v = threadIdx.x; v < 262144; v += blockDim.x) {
+    const float *r = g.levels[0].valueRange + 2 * ((uint64_t)v * g.numAttributes + attr);
+    lo             = fminx(lo, r[0]);
+    hi             = fmaxx(hi, r[1]);
+  }
+  __shared__ float slo[1024], shi[1024];
+  slo[threadIdx.x] = lo;
+  shi[threadIdx.x] = hi;
+  __syncthreads();
+  for (int s = 512; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      slo[threadIdx.x] = fminx(slo[threadIdx.x], slo[threadIdx.x + s]);
+      shi[threadIdx.x] = fmaxx(shi[threadIdx.x], shi[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = slo[0];
+    out[1] = shi[0];
+  }
+}
+
+inline unsigned blocksFor(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint64_t *vox2,
+                          uint32_t *org1, uint32_t *org2, const uint32_t nl[3],
+                          const uint32_t n1[3], const uint32_t n2[3], cudaStream_t st)
+{
+  (void)g;
+  const uint3 NL = {nl[0], nl[1], nl[2]}, N1 = {n1[0], n1[1], n1[2]}, N2 = {n2[0], n2[1], n2[2]};
+  const uint64_t t2 = (uint64_t)n2[0] * n2[1] * n2[2] * 4096;
+  const uint64_t t1 = (uint64_t)n1[0] * n1[1] * n1[2] * 32768;
+  kDenseLevel2<<<blocksFor(t2, 256), 256, 0, st>>>(vox2, org2, NL, N2);
+  kDenseLevel1<<<blocksFor(t1, 256), 256, 0, st>>>(vox1, org1, N2, N1);
+  kDenseLevel0<<<blocksFor(262144, 256), 256, 0, st>>>(vox0, N1);
+  cudaCheck(cudaGetLastError(), "dense tree kernels");
+}
+
+void launchDenseLeafRanges(const DevGrid &g, uint32_t attr, const uint32_t nl[3],
+                           float *leafRanges, float *scratch, cudaStream_t st)
+{
+  (void)scratch;
+  const uint3 NL      = {nl[0], nl[1], nl[2]};
+  const uint64_t n    = (uint64_t)nl[0] * nl[1] * nl[2];
+  const unsigned grid = blocksFor(n, 256);
+  switch (g.type[attr]) {
+  case kUChar:
+    kDenseLeafRanges<uint8_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    break;
+  case kShort:
+    kDenseLeafRanges<int16_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    break;
+  case kUShort:
+    kDenseLeafRanges<uint16_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    break;
+  case kHalf:
+    kDenseLeafRanges<__half><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    break;
+  case kDouble:
+    kDenseLeafRanges<double><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    break;
+  default:
+    kDenseLeafRanges<float><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+  }
+  cudaCheck(cudaGetLastError(), "dense leaf range kernel");
+}
+
+void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
+                            const uint32_t *leafOffsets, float *leafRanges, cudaStream_t st)
+{
+  const unsigned grid = blocksFor(numLeaves, 128);
+  if (g.type[attr] == kHalf)
+    kSparseLeafRanges<__half><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else
+    kSparseLeafRanges<float><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  cudaCheck(cudaGetLastError(), "sparse leaf range kernel");
+}
+
+void launchPropagateRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
+                           const uint64_t *leafVoxel, const float *leafRanges,
+                           float *volumeRange, const uint32_t nl[3], cudaStream_t st)
+{
+  if (attr == 0) {
+    for (uint32_t l = 0; l < kNumLevels - 1; ++l) {
+      const uint64_t n = g.levels[l].numNodes * levelNumVoxels(l) * g.numAttributes;
+      kFillEmpty<<<blocksFor(n, 256), 256, 0, st>>>((float *)g.levels[l].valueRange, n);
+    }
+  }
+  kLeafToParent<<<blocksFor(numLeaves, 256), 256, 0, st>>>(g, attr, numLeaves, leafVoxel,
+                                                           leafRanges, make_uint3(nl[0], nl[1], nl[2]));
+  for (uint32_t l = kNumLevels - 2; l >= 1; --l)
+    if (g.levels[l].numNodes)
+      kReduceNodes<<<(unsigned)g.levels[l].numNodes, 256, 0, st>>>(g, attr, l);
+  kVolumeRange<<<1, 1024, 0, st>>>(g, attr, volumeRange);
+  cudaCheck(cudaGetLastError(), "range propagation kernels");
+}
+
+}  // namespace vklcuda

@@ -1,0 +1,175 @@
+// Iterator kernels of the cuda device.  Batched forms run one thread per
+// ray through the whole DDA / hit loop; the per-call forms back the C API's
+// stateful vklIterateInterval / vklIterateHit by advancing a state struct
+// that lives in the caller's buffer by one step.
+#include "iterate.cuh"
+#include "kernels.h"
+#include "objects.h"
+
+namespace vklcuda {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ f3 ld3(const float *p, uint64_t i)
+{
+  return {__ldg(p + 3 * i), __ldg(p + 3 * i + 1), __ldg(p + 3 * i + 2)};
+}
+
+__global__ void __launch_bounds__(kBlock) kIntervals(const __grid_constant__ DevGrid g,
+                                                     uint32_t attr, uint32_t depth,
+                                                     DevValueRanges vr, uint64_t n,
+                                                     const float *__restrict__ orgs,
+                                                     const float *__restrict__ dirs,
+                                                     const float *__restrict__ tr,
+                                                     uint32_t maxPerRay,
+                                                     DevInterval *__restrict__ out,
+                                                     uint32_t *__restrict__ counts)
+{
+  const uint64_t r = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (r >= n)
+    return;
+  IntervalIt it;
+  intervalInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), it);
+  uint32_t c = 0;
+  DevInterval iv;
+  while (intervalNext(g, attr, vr, it, iv)) {
+    if (c < maxPerRay)
+      out[r * maxPerRay + c] = iv;
+    ++c;
+  }
+  counts[r] = c;
+}
+
+__global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid g, uint32_t attr,
+                                                int filter, uint32_t depth, DevValueRanges vr,
+                                                uint32_t numValues,
+                                                const float *__restrict__ values, uint64_t n,
+                                                const float *__restrict__ orgs,
+                                                const float *__restrict__ dirs,
+                                                const float *__restrict__ tr,
+                                                uint32_t maxPerRay, DevHit *__restrict__ out,
+                                                uint32_t *__restrict__ counts)
+{
+  const uint64_t r = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (r >= n)
+    return;
+  HitIt h;
+  hitInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), h);
+  uint32_t c = 0;
+  DevHit hit;
+  while (hitNext(g, filter, attr, kNumLevels - 1, vr, numValues, values, h, hit)) {
+    if (c < maxPerRay)
+      out[r * maxPerRay + c] = hit;
+    ++c;
+  }
+  counts[r] = c;
+}
+
+struct IntervalIterStateImpl {
+  uint32_t attr;
+  IntervalIt it;
+};
+struct HitIterStateImpl {
+  uint32_t attr;
+  HitIt h;
+};
+
+__global__ void kIntervalIterInit(const __grid_constant__ DevGrid g, uint32_t attr, uint32_t depth,
+                                  const float *ray, IntervalIterStateImpl *s)
+{
+  s->attr = attr;
+  intervalInit(g, depth, {ray[0], ray[1], ray[2]}, {ray[3], ray[4], ray[5]}, ray[6], ray[7], s->it);
+}
+
+__global__ void kIntervalIterNext(const __grid_constant__ DevGrid g, DevValueRanges vr,
+                                  IntervalIterStateImpl *s, DevInterval *out, int *result)
+{
+  DevInterval iv;
+  const bool ok = intervalNext(g, s->attr, vr, s->it, iv);
+  if (ok)
+    *out = iv;
+  *result = ok ? 1 : 0;
+}
+
+__global__ void kHitIterInit(const __grid_constant__ DevGrid g, uint32_t attr, uint32_t depth,
+                             const float *ray, HitIterStateImpl *s)
+{
+  s->attr = attr;
+  hitInit(g, depth, {ray[0], ray[1], ray[2]}, {ray[3], ray[4], ray[5]}, ray[6], ray[7], s->h);
+}
+
+__global__ void kHitIterNext(const __grid_constant__ DevGrid g, int filter, DevValueRanges vr,
+                             uint32_t numValues, const float *values, HitIterStateImpl *s,
+                             DevHit *out, int *result)
+{
+  DevHit hit;
+  const bool ok = hitNext(g, filter, s->attr, kNumLevels - 1, vr, numValues, values, s->h, hit);
+  if (ok)
+    *out = hit;
+  *result = ok ? 1 : 0;
+}
+
+inline unsigned blocksFor(uint64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+void launchIntervals(const DevGrid &g, uint32_t attr, uint32_t depth, DevValueRanges vr,
+                     uint64_t n, const float *origins, const float *directions,
+                     const float *tRanges, uint32_t maxPerRay, DevInterval *out,
+                     uint32_t *counts, cudaStream_t st)
+{
+  if (!n)
+    return;
+  kIntervals<<<blocksFor(n), kBlock, 0, st>>>(g, attr, depth, vr, n, origins, directions, tRanges,
+                                               maxPerRay, out, counts);
+  cudaCheck(cudaGetLastError(), "interval kernel launch");
+}
+
+void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, DevValueRanges vr,
+                uint32_t numValues, const float *values, uint64_t n, const float *origins,
+                const float *directions, const float *tRanges, uint32_t maxPerRay, DevHit *out,
+                uint32_t *counts, cudaStream_t st)
+{
+  if (!n)
+    return;
+  kHits<<<blocksFor(n), kBlock, 0, st>>>(g, attr, filter, depth, vr, numValues, values, n, origins,
+                                          directions, tRanges, maxPerRay, out, counts);
+  cudaCheck(cudaGetLastError(), "hit kernel launch");
+}
+
+size_t intervalIterStateSize() { return sizeof(IntervalIterStateImpl); }
+size_t hitIterStateSize() { return sizeof(HitIterStateImpl); }
+
+void launchIntervalIterInit(const DevGrid &g, uint32_t attr, uint32_t depth, const float *ray,
+                            void *state, cudaStream_t st)
+{
+  kIntervalIterInit<<<1, 1, 0, st>>>(g, attr, depth, ray, (IntervalIterStateImpl *)state);
+  cudaCheck(cudaGetLastError(), "interval iterator init");
+}
+
+void launchIntervalIterNext(const DevGrid &g, DevValueRanges vr, void *state, DevInterval *out,
+                            int *result, cudaStream_t st)
+{
+  kIntervalIterNext<<<1, 1, 0, st>>>(g, vr, (IntervalIterStateImpl *)state, out, result);
+  cudaCheck(cudaGetLastError(), "interval iterator step");
+}
+
+void launchHitIterInit(const DevGrid &g, uint32_t attr, uint32_t depth, const float *ray,
+                       void *state, cudaStream_t st)
+{
+  kHitIterInit<<<1, 1, 0, st>>>(g, attr, depth, ray, (HitIterStateImpl *)state);
+  cudaCheck(cudaGetLastError(), "hit iterator init");
+}
+
+void launchHitIterNext(const DevGrid &g, int filter, DevValueRanges vr, uint32_t numValues,
+                       const float *values, void *state, DevHit *out, int *result,
+                       cudaStream_t st)
+{
+  kHitIterNext<<<1, 1, 0, st>>>(g, filter, vr, numValues, values, (HitIterStateImpl *)state, out,
+                                result);
+  cudaCheck(cudaGetLastError(), "hit iterator step");
+}
+
+}  // namespace vklcuda

@@ -1,0 +1,7 @@
+// linear filter instantiation of the sampling kernels (sample_kernels.cuh).
+#include "sample_kernels.cuh"
+
+namespace vklcuda {
+template void dispatchFilter<kFilterLinear>(const DevGrid &, uint32_t, uint64_t, const float *, uint32_t,
+                                  float *, bool, cudaStream_t);
+}  // namespace vklcuda

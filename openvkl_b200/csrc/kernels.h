@@ -1,0 +1,72 @@
+// Host-callable launchers of the cuda device's kernels.  All pointers are
+// device pointers; every launcher enqueues on `stream` and returns without
+// synchronizing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "grid.h"
+
+namespace vklcuda {
+
+// Sampling / gradients over N object-space points (AoS float3).  `attrs`
+// lists M attribute indices (M <= kMaxAttributes, host array); output is
+// out[i*M + m] for samples and out[3*i ...] for gradients (M == 1).
+void launchSample(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
+                  const float *points, uint32_t M, const uint32_t *attrs, float *out,
+                  cudaStream_t stream);
+void launchGradient(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
+                    const float *points, uint32_t attr, float *out, cudaStream_t stream);
+
+// Commit-time tree construction for dense volumes: fills the voxel codes and
+// node origins of levels 0..2 (closed form of the reference's insertion
+// order for x-fastest leaves).
+void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint64_t *vox2,
+                          uint32_t *org1, uint32_t *org2, const uint32_t nl[3],
+                          const uint32_t n1[3], const uint32_t n2[3], cudaStream_t stream);
+
+// Per-leaf value ranges (2 floats per leaf per attribute) of dense volumes:
+// min/max over each leaf's 3x3x3-leaf filter neighbourhood window.
+void launchDenseLeafRanges(const DevGrid &g, uint32_t attr, const uint32_t nl[3],
+                           float *leafRanges, float *scratch, cudaStream_t stream);
+// Same for sparse volumes, leaves given by root-relative offsets (3 u32).
+void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
+                            const uint32_t *leafOffsets, float *leafRanges,
+                            cudaStream_t stream);
+// Writes leaf ranges into the parent voxels (leafVoxel[i] = level*2^40 +
+// voxel index on that level, ~0 to skip; NULL for dense volumes, whose
+// parents follow from the leaf counts nl), then reduces level 2 -> 1 -> 0
+// child nodes into their parent voxels, and the level-0 node into
+// volumeRange.  Attribute 0's call first resets all ranges to empty.
+void launchPropagateRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
+                           const uint64_t *leafVoxel, const float *leafRanges,
+                           float *volumeRange, const uint32_t nl[3], cudaStream_t stream);
+
+// Batched interval iteration: one thread per ray.
+void launchIntervals(const DevGrid &g, uint32_t attr, uint32_t depth, DevValueRanges vr,
+                     uint64_t n, const float *origins, const float *directions,
+                     const float *tRanges, uint32_t maxPerRay, DevInterval *out,
+                     uint32_t *counts, cudaStream_t stream);
+// Batched hit iteration: one thread per ray.
+void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, DevValueRanges vr,
+                uint32_t numValues, const float *values, uint64_t n, const float *origins,
+                const float *directions, const float *tRanges, uint32_t maxPerRay,
+                DevHit *out, uint32_t *counts, cudaStream_t stream);
+
+// Per-ray stateful iterators of the C API: the state lives in the caller's
+// buffer; each call advances it on the GPU by one interval / hit.
+struct IntervalIterState;
+struct HitIterState;
+size_t intervalIterStateSize();
+size_t hitIterStateSize();
+void launchIntervalIterInit(const DevGrid &g, uint32_t attr, uint32_t depth, const float *ray,
+                            void *state, cudaStream_t stream);
+void launchIntervalIterNext(const DevGrid &g, DevValueRanges vr, void *state,
+                            DevInterval *out, int *result, cudaStream_t stream);
+void launchHitIterInit(const DevGrid &g, uint32_t attr, uint32_t depth, const float *ray,
+                       void *state, cudaStream_t stream);
+void launchHitIterNext(const DevGrid &g, int filter, DevValueRanges vr, uint32_t numValues,
+                       const float *values, void *state, DevHit *out, int *result,
+                       cudaStream_t stream);
+
+}  // namespace vklcuda

@@ -1,0 +1,286 @@
+// Host object model of the cuda device: devices, data arrays, volumes,
+// samplers, iterator contexts and observers, with the reference's parameter
+// and reference-counting semantics (openvkl/common/ManagedObject.h,
+// openvkl/api/Device.h:42-185).  Errors are C++ exceptions inside the
+// library and are turned into the device's last-error code / message and
+// error callback at the C boundary (api.cpp), as the reference does
+// (openvkl/api/API.cpp:37-89).  Commit-time validation errors carry
+// VKL_UNKNOWN_ERROR (1) like the reference's runtimeError() throws.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/openvkl_cuda.h"
+#include "grid.h"
+
+namespace vklcuda {
+
+struct VklError : std::runtime_error {
+  VKLError code;
+  VklError(VKLError c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(const std::string &msg, VKLError code = VKL_UNKNOWN_ERROR)
+{
+  throw VklError(code, msg);
+}
+
+inline void cudaCheck(cudaError_t e, const char *what)
+{
+  if (e != cudaSuccess)
+    fail(std::string(what) + ": " + cudaGetErrorString(e),
+         e == cudaErrorMemoryAllocation ? VKL_OUT_OF_MEMORY : VKL_UNKNOWN_ERROR);
+}
+
+size_t sizeOfType(VKLDataType t);
+
+struct Device;
+
+// ---------------------------------------------------------------------------
+// Reference-counted object with a parameter table.
+// ---------------------------------------------------------------------------
+struct ManagedObject {
+  std::atomic<int> refs{1};
+  Device *device = nullptr;
+
+  struct Param {
+    VKLDataType type = VKL_UNKNOWN;
+    std::vector<uint8_t> bytes;
+    std::string str;
+    ManagedObject *obj = nullptr;
+  };
+  std::map<std::string, Param> params;
+
+  virtual ~ManagedObject();
+  virtual void commit() {}
+  virtual const char *typeName() const = 0;
+
+  void refInc() { refs.fetch_add(1); }
+  void refDec()
+  {
+    if (refs.fetch_sub(1) == 1)
+      delete this;
+  }
+
+  void setParam(const char *name, VKLDataType type, const void *mem);
+  bool has(const std::string &name) const { return params.count(name) != 0; }
+  const Param *find(const std::string &name) const
+  {
+    auto it = params.find(name);
+    return it == params.end() ? nullptr : &it->second;
+  }
+  int getInt(const std::string &name, int def) const;
+  float getFloat(const std::string &name, float def) const;
+  bool getBool(const std::string &name, bool def) const;
+  void getVec3f(const std::string &name, float out[3], const float def[3]) const;
+  void getVec3i(const std::string &name, int out[3], const int def[3]) const;
+  struct Data *getData(const std::string &name) const;
+};
+
+template <class T>
+struct Ref {
+  T *p = nullptr;
+  Ref() = default;
+  explicit Ref(T *x) : p(x)
+  {
+    if (p)
+      p->refInc();
+  }
+  Ref(const Ref &o) : p(o.p)
+  {
+    if (p)
+      p->refInc();
+  }
+  Ref &operator=(const Ref &o)
+  {
+    if (o.p)
+      o.p->refInc();
+    if (p)
+      p->refDec();
+    p = o.p;
+    return *this;
+  }
+  ~Ref()
+  {
+    if (p)
+      p->refDec();
+  }
+  T *operator->() const { return p; }
+  T &operator*() const { return *p; }
+  explicit operator bool() const { return p != nullptr; }
+};
+
+// ---------------------------------------------------------------------------
+// Device memory owned by an object.
+// ---------------------------------------------------------------------------
+struct DeviceBuffer {
+  void *ptr    = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  ~DeviceBuffer() { release(); }
+  void release()
+  {
+    if (ptr)
+      cudaFree(ptr);
+    ptr   = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t n)
+  {
+    release();
+    if (n) {
+      cudaCheck(cudaMalloc(&ptr, n), "cudaMalloc");
+      bytes = n;
+    }
+  }
+  // Grow-only (scratch use).
+  void reserve(size_t n)
+  {
+    if (n > bytes)
+      alloc(n + n / 4);
+  }
+  template <class T>
+  T *as() const
+  {
+    return (T *)ptr;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Device.
+// ---------------------------------------------------------------------------
+struct Device {
+  int cudaDevice = 0;
+  cudaStream_t stream = nullptr;
+  VKLError lastErrorCode = VKL_NO_ERROR;
+  std::string lastErrorMsg;
+  VKLErrorCallback errorCb = nullptr;
+  void *errorUser = nullptr;
+  VKLLogCallback logCb = nullptr;
+  void *logUser = nullptr;
+  int logLevel = VKL_LOG_WARNING;
+  bool committed = false;
+  std::map<std::string, int> intParams;
+  std::map<std::string, std::string> stringParams;
+
+  // Staging memory for host-pointer calls; guarded by `stagingMutex`.
+  std::mutex stagingMutex;
+  DeviceBuffer stageIn, stageOut, stageAux;
+
+  void setError(VKLError code, const std::string &msg);
+  void log(int level, const std::string &msg);
+};
+
+// ---------------------------------------------------------------------------
+// Data arrays (openvkl/common/Data.h): always held compact in device memory
+// (strided sources are compacted on upload); a host copy is kept for the
+// small metadata arrays the commit logic reads on the host.
+// ---------------------------------------------------------------------------
+struct Data : ManagedObject {
+  VKLDataType type = VKL_UNKNOWN;
+  size_t numItems  = 0;
+  size_t itemSize  = 0;
+  const void *dev  = nullptr;  // compact device array
+  DeviceBuffer owned;
+  std::vector<uint8_t> host;   // compact host copy (may be empty)
+  std::vector<ManagedObject *> objects;  // object arrays (VKL_DATA etc.)
+
+  ~Data() override;
+  const char *typeName() const override { return "Data"; }
+  // Compact host bytes (copied back from the device on first use).
+  const uint8_t *hostBytes();
+  template <class T>
+  const T *hostAs()
+  {
+    return (const T *)hostBytes();
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Volumes.
+// ---------------------------------------------------------------------------
+struct Volume : ManagedObject {
+  bool isDense = false;
+  bool committed = false;
+  DevGrid grid{};
+  std::vector<std::unique_ptr<DeviceBuffer>> buffers;
+  std::vector<Ref<Data>> keep;   // data referenced by the grid
+  std::vector<float> rangeLo, rangeHi;  // per attribute
+  vkl_box3f bounds{};
+  int filter = VKL_FILTER_LINEAR;
+  int gradientFilter = VKL_FILTER_LINEAR;
+  uint32_t maxSamplingDepth = kNumLevels - 1;
+  uint64_t levelNodes[kNumLevels] = {0, 0, 0, 0};
+
+  const char *typeName() const override { return isDense ? "structuredRegular" : "vdb"; }
+  void commit() override;
+  DeviceBuffer *newBuffer(size_t bytes)
+  {
+    buffers.emplace_back(new DeviceBuffer());
+    buffers.back()->alloc(bytes);
+    return buffers.back().get();
+  }
+
+ private:
+  void commitDense();
+  void commitVdb();
+  void finishCommit(const float indexLo[3], const float indexHi[3]);
+};
+
+struct Sampler : ManagedObject {
+  Ref<Volume> volume;
+  DevSampler s{};
+  DeviceBuffer devState;  // {DevGrid, DevSampler} for the device-side API
+  const char *typeName() const override { return "Sampler"; }
+  void commit() override;
+};
+
+struct IntervalContext : ManagedObject {
+  Ref<Sampler> sampler;
+  uint32_t attr = 0;
+  std::vector<float> ranges;  // 2 per range
+  float minMax[2]   = {0, 0};
+  uint32_t depth    = 2;
+  bool elementary   = false;
+  DeviceBuffer devRanges;
+  const char *typeName() const override { return "IntervalIteratorContext"; }
+  void commit() override;
+  DevValueRanges devValueRanges() const;
+};
+
+struct HitContext : ManagedObject {
+  Ref<Sampler> sampler;
+  uint32_t attr = 0;
+  std::vector<float> values;
+  std::vector<float> ranges;
+  float minMax[2] = {0, 0};
+  uint32_t depth  = 2;
+  DeviceBuffer devRanges, devValues;
+  const char *typeName() const override { return "HitIteratorContext"; }
+  void commit() override;
+  DevValueRanges devValueRanges() const;
+};
+
+struct Observer : ManagedObject {
+  Ref<Volume> volume;
+  Ref<Sampler> sampler;
+  std::string kind;
+  std::vector<float> buffer;
+  size_t elementFloats = 0;
+  size_t numElements   = 0;
+  std::vector<uint32_t> leafAccess;  // LeafNodeAccess counters (host copy)
+  DeviceBuffer devCounters;
+  const char *typeName() const override { return "Observer"; }
+  void commit() override;
+};
+
+}  // namespace vklcuda

@@ -1,0 +1,457 @@
+// Device-side field access and reconstruction filters of the cuda device.
+//
+// Arithmetic follows the reference CPU device's float expressions operation
+// by operation (the translation unit is built with --fmad=false so nothing is
+// contracted into an FMA that the source does not spell out):
+//   transforms      VdbGrid.h:56-89 (xfmPoint / xfmNormal)
+//   nearest         VdbSampler_nearest.ih:15-57
+//   trilinear       VdbSampler_trilinear.ih:378-399, gradient :751-780
+//   tricubic        VdbSampler_tricubic.ih:34-580 (Lekien-Marsden map)
+//   dense taps      VdbSampler_traverseAndSample.ih:313-349
+//   sparse taps     VdbSampler_traverseAndSample.ih:85-306 with the
+//                   generated per-level walk VdbSampleInner.ih.in:33-76
+//   packed leaves   VdbSampler_packed_denseZYX.ih:77-187, _packed_tile.ih
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+#include <stdint.h>
+
+#include "grid.h"
+
+namespace vklcuda {
+
+struct f3 {
+  float x, y, z;
+};
+
+// rkcommon lerp: (1 - f) * a + f * b.
+__device__ __forceinline__ float lerpf(float f, float a, float b)
+{
+  return (1.f - f) * a + f * b;
+}
+
+// float -> int32 the way x86 cvttss2si does it (the CPU device's floor
+// results go through it): NaN and out-of-range values give INT32_MIN.
+__device__ __forceinline__ int32_t toIntX86(float x)
+{
+  return (x >= -2147483648.f && x < 2147483648.f) ? (int32_t)x : INT32_MIN;
+}
+__device__ __forceinline__ int32_t ifloor(float x) { return toIntX86(floorf(x)); }
+
+__device__ __forceinline__ f3 xfmPoint(const float *M, f3 p)
+{
+  return {M[0] * p.x + M[1] * p.y + M[2] * p.z + M[9],
+          M[3] * p.x + M[4] * p.y + M[5] * p.z + M[10],
+          M[6] * p.x + M[7] * p.y + M[8] * p.z + M[11]};
+}
+__device__ __forceinline__ f3 xfmVector(const float *M, f3 p)
+{
+  return {M[0] * p.x + M[1] * p.y + M[2] * p.z, M[3] * p.x + M[4] * p.y + M[5] * p.z,
+          M[6] * p.x + M[7] * p.y + M[8] * p.z};
+}
+__device__ __forceinline__ f3 xfmNormal(const float *Mi, f3 p)
+{
+  return {Mi[0] * p.x + Mi[3] * p.y + Mi[6] * p.z, Mi[1] * p.x + Mi[4] * p.y + Mi[7] * p.z,
+          Mi[2] * p.x + Mi[5] * p.y + Mi[8] * p.z};
+}
+
+// ---------------------------------------------------------------------------
+// Typed loads (read-only path).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ float ldv(const T *p, uint64_t i);
+template <>
+__device__ __forceinline__ float ldv<float>(const float *p, uint64_t i)
+{
+  return __ldg(p + i);
+}
+template <>
+__device__ __forceinline__ float ldv<uint8_t>(const uint8_t *p, uint64_t i)
+{
+  return (float)__ldg(p + i);
+}
+template <>
+__device__ __forceinline__ float ldv<int16_t>(const int16_t *p, uint64_t i)
+{
+  return (float)__ldg(p + i);
+}
+template <>
+__device__ __forceinline__ float ldv<uint16_t>(const uint16_t *p, uint64_t i)
+{
+  return (float)__ldg(p + i);
+}
+template <>
+__device__ __forceinline__ float ldv<__half>(const __half *p, uint64_t i)
+{
+  return __half2float(__ldg(p + i));
+}
+template <>
+__device__ __forceinline__ float ldv<double>(const double *p, uint64_t i)
+{
+  return __double2float_rn(__ldg(p + i));
+}
+
+__device__ __forceinline__ float ldAny(uint32_t type, const void *p, uint64_t i)
+{
+  switch (type) {
+  case kUChar:
+    return ldv((const uint8_t *)p, i);
+  case kShort:
+    return ldv((const int16_t *)p, i);
+  case kUShort:
+    return ldv((const uint16_t *)p, i);
+  case kHalf:
+    return ldv((const __half *)p, i);
+  case kDouble:
+    return ldv((const double *)p, i);
+  default:
+    return ldv((const float *)p, i);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense field: x-fastest array, out-of-domain taps read the background.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DenseField {
+  const T *data;
+  uint32_t ax, ay, az;
+  int32_t rx, ry, rz;
+  float bg;
+
+  __device__ __forceinline__ DenseField(const DevGrid &g, uint32_t a)
+      : data((const T *)g.data[a]),
+        ax(g.activeSize[0]),
+        ay(g.activeSize[1]),
+        az(g.activeSize[2]),
+        rx(g.rootOrigin[0]),
+        ry(g.rootOrigin[1]),
+        rz(g.rootOrigin[2]),
+        bg(g.background[a])
+  {
+  }
+
+  __device__ __forceinline__ float at(int32_t x, int32_t y, int32_t z) const
+  {
+    const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
+    if (ox < ax && oy < ay && oz < az)
+      return ldv(data, ((uint64_t)oz * ay + oy) * (uint64_t)ax + ox);
+    return bg;
+  }
+
+  // The 8 trilinear corners s[4x+2y+z] at (x..x+1, y..y+1, z..z+1).
+  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  {
+    const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
+    if (ox + 1 < ax && oy + 1 < ay && oz + 1 < az && ox < ax && oy < ay && oz < az) {
+      const uint64_t sy = ax, sz = (uint64_t)ax * ay;
+      const T *b = data + (oz * sz + oy * sy + ox);
+      s[0]       = ldv(b, 0);
+      s[4]       = ldv(b, 1);
+      s[2]       = ldv(b, sy);
+      s[6]       = ldv(b, sy + 1);
+      s[1]       = ldv(b, sz);
+      s[5]       = ldv(b, sz + 1);
+      s[3]       = ldv(b, sz + sy);
+      s[7]       = ldv(b, sz + sy + 1);
+    } else {
+#pragma unroll
+      for (int o = 0; o < 8; ++o)
+        s[o] = at(x + (o >> 2), y + ((o >> 1) & 1), z + (o & 1));
+    }
+  }
+
+  // The 64 tricubic taps s[16x+4y+z] at offsets -1..2.
+  __device__ __forceinline__ void stencil64(int32_t x, int32_t y, int32_t z, float s[64]) const
+  {
+    const uint32_t ox = (uint32_t)(x - 1 - rx), oy = (uint32_t)(y - 1 - ry),
+                   oz = (uint32_t)(z - 1 - rz);
+    if (ox + 3 < ax && oy + 3 < ay && oz + 3 < az && ox < ax && oy < ay && oz < az) {
+      const uint64_t sy = ax, sz = (uint64_t)ax * ay;
+      const T *b = data + (oz * sz + oy * sy + ox);
+#pragma unroll
+      for (int o = 0; o < 64; ++o)
+        s[o] = ldv(b, (uint64_t)(o & 3) * sz + (uint64_t)((o >> 2) & 3) * sy + (o >> 4));
+    } else {
+#pragma unroll
+      for (int o = 0; o < 64; ++o)
+        s[o] = at(x + (o >> 4) - 1, y + ((o >> 2) & 3) - 1, z + (o & 3) - 1);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Sparse field: 4-level tree walk, packed leaves, tiles, error voxels.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct SparseField {
+  const DevGrid &g;
+  uint32_t attr;
+  uint32_t maxDepth;
+
+  __device__ __forceinline__ SparseField(const DevGrid &grid, uint32_t a, uint32_t depth)
+      : g(grid), attr(a), maxDepth(depth)
+  {
+  }
+
+  // Walk from the root to the voxel holding the leaf that contains the
+  // (in-domain, root-relative) offset.
+  __device__ __forceinline__ uint64_t traverse(uint32_t ox, uint32_t oy, uint32_t oz) const
+  {
+    const uint32_t lx = ox & ~7u, ly = oy & ~7u, lz = oz & ~7u;
+    uint64_t node = 0;
+#pragma unroll
+    for (uint32_t l = 0; l < kNumLevels - 1; ++l) {
+      const uint64_t vo   = node * levelNumVoxels(l) + offsetToLinear(l, lx, ly, lz);
+      const uint32_t vo32 = (uint32_t)vo;
+      const uint64_t v    = __ldg(g.levels[l].voxels + vo32);
+      if ((voxelIsLeaf(v) || voxelIsChild(v)) && (l + 1 > maxDepth))
+        return voxelMakeError(l, vo32);
+      if (voxelIsChild(v) && l + 1 < kNumLevels - 1) {
+        node = voxelChildIndex(v);
+        continue;
+      }
+      return v;
+    }
+    return 0;
+  }
+
+  __device__ __forceinline__ float leafValue(uint64_t voxel, uint32_t ox, uint32_t oy,
+                                             uint32_t oz) const
+  {
+    if (voxelIsLeaf(voxel)) {
+      const uint64_t li = voxelLeafIndex(voxel);
+      if (voxelLeafFormat(voxel) == kFormatTile)
+        return ldv((const T *)g.tile[attr], li);
+      const uint64_t vi = li * 512 + ((uint64_t)(ox & 7u) << 6) + ((oy & 7u) << 3) + (oz & 7u);
+      return ldv((const T *)g.data[attr], vi);
+    } else if (voxelIsError(voxel)) {
+      const uint32_t level = (uint32_t)((voxel >> 8) & 0xffu);
+      const uint32_t off   = (uint32_t)(voxel >> 32);
+      const float *r = g.levels[level].valueRange + 2 * ((uint64_t)off * g.numAttributes + attr);
+      return 0.5f * (__ldg(r) + __ldg(r + 1));
+    } else if (!(ox < g.activeSize[0] && oy < g.activeSize[1] && oz < g.activeSize[2])) {
+      return g.background[attr];
+    }
+    return 0.f;
+  }
+
+  __device__ __forceinline__ bool inDomain(uint32_t ox, uint32_t oy, uint32_t oz) const
+  {
+    return ox < g.activeSize[0] && oy < g.activeSize[1] && oz < g.activeSize[2];
+  }
+
+  __device__ __forceinline__ float at(int32_t x, int32_t y, int32_t z) const
+  {
+    const uint32_t ox = (uint32_t)(x - g.rootOrigin[0]), oy = (uint32_t)(y - g.rootOrigin[1]),
+                   oz = (uint32_t)(z - g.rootOrigin[2]);
+    if (!inDomain(ox, oy, oz))
+      return g.background[attr];
+    return leafValue(traverse(ox, oy, oz), ox, oy, oz);
+  }
+
+  // Taps of a stencil spanning offsets [lo, lo+W) per axis reuse one walk
+  // per distinct leaf: the walk result depends only on the leaf origin
+  // (offset & ~7), and W <= 8 means at most two leaves per axis.
+  template <int W, int LO>
+  __device__ __forceinline__ void stencil(int32_t x, int32_t y, int32_t z, float *s) const
+  {
+    const uint32_t bx = (uint32_t)(x + LO - g.rootOrigin[0]),
+                   by = (uint32_t)(y + LO - g.rootOrigin[1]),
+                   bz = (uint32_t)(z + LO - g.rootOrigin[2]);
+    uint64_t cache[8];
+    uint32_t have = 0;
+#pragma unroll
+    for (int o = 0; o < W * W * W; ++o) {
+      const int dx = o / (W * W), dy = (o / W) % W, dz = o % W;
+      const uint32_t ox = bx + dx, oy = by + dy, oz = bz + dz;
+      if (!inDomain(ox, oy, oz)) {
+        s[o] = g.background[attr];
+        continue;
+      }
+      const uint32_t slot = (((ox & ~7u) != (bx & ~7u)) << 2) |
+                            (((oy & ~7u) != (by & ~7u)) << 1) | ((oz & ~7u) != (bz & ~7u));
+      if (!(have & (1u << slot))) {
+        cache[slot] = traverse(ox, oy, oz);
+        have |= 1u << slot;
+      }
+      s[o] = leafValue(cache[slot], ox, oy, oz);
+    }
+  }
+
+  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  {
+    stencil<2, 0>(x, y, z, s);
+  }
+  __device__ __forceinline__ void stencil64(int32_t x, int32_t y, int32_t z, float s[64]) const
+  {
+    stencil<4, -1>(x, y, z, s);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Filters.
+// ---------------------------------------------------------------------------
+template <class Field>
+__device__ __forceinline__ float sampleNearest(const Field &F, bool cellCentered, f3 p)
+{
+  const float off = cellCentered ? 0.f : 0.5f;
+  return F.at(ifloor(p.x + off), ifloor(p.y + off), ifloor(p.z + off));
+}
+
+template <class Field>
+__device__ __forceinline__ float sampleLinear(const Field &F, f3 p)
+{
+  const int32_t ix = ifloor(p.x), iy = ifloor(p.y), iz = ifloor(p.z);
+  const float dx = p.x - (float)ix, dy = p.y - (float)iy, dz = p.z - (float)iz;
+  float s[8];
+  F.corners(ix, iy, iz, s);
+  return lerpf(dx, lerpf(dy, lerpf(dz, s[0], s[1]), lerpf(dz, s[2], s[3])),
+               lerpf(dy, lerpf(dz, s[4], s[5]), lerpf(dz, s[6], s[7])));
+}
+
+template <class Field>
+__device__ __forceinline__ f3 gradientLinear(const Field &F, f3 p)
+{
+  const int32_t ix = ifloor(p.x), iy = ifloor(p.y), iz = ifloor(p.z);
+  const float dx = p.x - (float)ix, dy = p.y - (float)iy, dz = p.z - (float)iz;
+  float s[8];
+  F.corners(ix, iy, iz, s);
+  f3 r;
+  r.x = lerpf(dy, lerpf(dz, s[4] - s[0], s[5] - s[1]), lerpf(dz, s[6] - s[2], s[7] - s[3]));
+  r.y = lerpf(dx, lerpf(dz, s[2] - s[0], s[3] - s[1]), lerpf(dz, s[6] - s[4], s[7] - s[5]));
+  r.z = lerpf(dx, lerpf(dy, s[1] - s[0], s[3] - s[2]), lerpf(dy, s[5] - s[4], s[7] - s[6]));
+  return r;
+}
+
+// Lekien-Marsden tricubic: constraints from central differences, then the
+// 64x64 coefficient map.  The map is the tensor product of the 1D cubic
+// Hermite map; its non-zero entries, summed per row in ascending column order
+// exactly as the reference's expanded expressions are, live in
+// tricubic_map.cuh (generated, with a test that pins it to the reference).
+#include "tricubic_map.cuh"
+
+__device__ __forceinline__ void tricubicCoefficients(const float s[64], float coef[64])
+{
+#define S(X, Y, Z) s[((X) + 1) * 16 + ((Y) + 1) * 4 + ((Z) + 1)]
+  float ctr[64];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int x = c >> 2, y = (c >> 1) & 1, z = c & 1;
+    ctr[c]      = S(x, y, z);
+    ctr[8 + c]  = 0.5f * (-S(x - 1, y, z) + S(x + 1, y, z));
+    ctr[16 + c] = 0.5f * (-S(x, y - 1, z) + S(x, y + 1, z));
+    ctr[24 + c] = 0.5f * (-S(x, y, z - 1) + S(x, y, z + 1));
+    ctr[32 + c] = 0.25f * (S(x - 1, y - 1, z) - S(x - 1, y + 1, z) - S(x + 1, y - 1, z) +
+                           S(x + 1, y + 1, z));
+    ctr[40 + c] = 0.25f * (S(x - 1, y, z - 1) - S(x - 1, y, z + 1) - S(x + 1, y, z - 1) +
+                           S(x + 1, y, z + 1));
+    ctr[48 + c] = 0.25f * (S(x, y - 1, z - 1) - S(x, y - 1, z + 1) - S(x, y + 1, z - 1) +
+                           S(x, y + 1, z + 1));
+    ctr[56 + c] = 0.125f * (-S(x - 1, y - 1, z - 1) + S(x - 1, y - 1, z + 1) +
+                            S(x - 1, y + 1, z - 1) - S(x - 1, y + 1, z + 1) +
+                            S(x + 1, y - 1, z - 1) - S(x + 1, y - 1, z + 1) -
+                            S(x + 1, y + 1, z - 1) + S(x + 1, y + 1, z + 1));
+  }
+#undef S
+  VKL_TRICUBIC_MAP(ctr, coef)
+}
+
+template <class Field>
+__device__ __forceinline__ float sampleCubic(const Field &F, f3 p)
+{
+  const int32_t ix = ifloor(p.x), iy = ifloor(p.y), iz = ifloor(p.z);
+  float s[64], c[64];
+  F.stencil64(ix, iy, iz, s);
+  tricubicCoefficients(s, c);
+  const float dx = p.x - (float)ix, dy = p.y - (float)iy, dz = p.z - (float)iz;
+  const float X[4] = {1.f, dx, dx * dx, dx * dx * dx};
+  const float Y[4] = {1.f, dy, dy * dy, dy * dy * dy};
+  const float Z[4] = {1.f, dz, dz * dz, dz * dz * dz};
+  float r = 0.f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        r += c[16 * i + 4 * j + k] * X[i] * Y[j] * Z[k];
+  return r;
+}
+
+template <class Field>
+__device__ __forceinline__ f3 gradientCubic(const Field &F, f3 p)
+{
+  const int32_t ix = ifloor(p.x), iy = ifloor(p.y), iz = ifloor(p.z);
+  float s[64], c[64];
+  F.stencil64(ix, iy, iz, s);
+  tricubicCoefficients(s, c);
+  const float dx = p.x - (float)ix, dy = p.y - (float)iy, dz = p.z - (float)iz;
+  const float X[4] = {1.f, dx, dx * dx, dx * dx * dx};
+  const float Y[4] = {1.f, dy, dy * dy, dy * dy * dy};
+  const float Z[4] = {1.f, dz, dz * dz, dz * dz * dz};
+  f3 r = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float cc = c[16 * i + 4 * j + k];
+        if (i > 0)
+          r.x += cc * (float)i * X[i - 1] * Y[j] * Z[k];
+        if (j > 0)
+          r.y += cc * (float)j * X[i] * Y[j - 1] * Z[k];
+        if (k > 0)
+          r.z += cc * (float)k * X[i] * Y[j] * Z[k - 1];
+      }
+  return r;
+}
+
+template <class Field>
+__device__ __forceinline__ float sampleFiltered(const Field &F, int filter, bool cellCentered, f3 p)
+{
+  if (filter == kFilterNearest)
+    return sampleNearest(F, cellCentered, p);
+  if (filter == kFilterCubic)
+    return sampleCubic(F, p);
+  return sampleLinear(F, p);
+}
+
+// Sample at an object-space point with runtime type dispatch (used by the
+// hit iterator's marching, VdbSampler_iterator_computeSample_varying,
+// VdbSampler.ispc:341-374).
+__device__ __forceinline__ float sampleIndexAny(const DevGrid &g, int filter, uint32_t attr,
+                                                uint32_t depth, f3 p)
+{
+  const bool cc = g.constantCellData != 0;
+  const uint32_t t = g.type[attr];
+  if (g.dense) {
+    switch (t) {
+    case kUChar:
+      return sampleFiltered(DenseField<uint8_t>(g, attr), filter, cc, p);
+    case kShort:
+      return sampleFiltered(DenseField<int16_t>(g, attr), filter, cc, p);
+    case kUShort:
+      return sampleFiltered(DenseField<uint16_t>(g, attr), filter, cc, p);
+    case kHalf:
+      return sampleFiltered(DenseField<__half>(g, attr), filter, cc, p);
+    case kDouble:
+      return sampleFiltered(DenseField<double>(g, attr), filter, cc, p);
+    default:
+      return sampleFiltered(DenseField<float>(g, attr), filter, cc, p);
+    }
+  }
+  if (t == kHalf)
+    return sampleFiltered(SparseField<__half>(g, attr, depth), filter, cc, p);
+  return sampleFiltered(SparseField<float>(g, attr, depth), filter, cc, p);
+}
+
+__device__ __forceinline__ float sampleObjectAny(const DevGrid &g, int filter, uint32_t attr,
+                                                 uint32_t depth, f3 oc)
+{
+  return sampleIndexAny(g, filter, attr, depth, xfmPoint(g.objectToIndex, oc));
+}
+
+}  // namespace vklcuda

@@ -1,0 +1,239 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+ctypes binding of oracle/build/liboracle.so, the C++ restatement of the
+Open VKL v2.0.2 CPU device's VDB / structuredRegular path (vkl_oracle.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product (openvkl_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(_HERE, "build")
+
+FILTER_NEAREST, FILTER_LINEAR, FILTER_CUBIC = 0, 100, 200
+T_UCHAR, T_SHORT, T_USHORT, T_HALF, T_FLOAT, T_DOUBLE = 2500, 3000, 3500, 5800, 6000, 7000
+_NP2VKL = {
+    np.dtype(np.uint8): T_UCHAR,
+    np.dtype(np.int16): T_SHORT,
+    np.dtype(np.uint16): T_USHORT,
+    np.dtype(np.float16): T_HALF,
+    np.dtype(np.float32): T_FLOAT,
+    np.dtype(np.float64): T_DOUBLE,
+}
+BACKGROUND_UNDEFINED = np.frombuffer(np.uint32(0xFFC068B5).tobytes(), np.float32)[0]
+
+
+def build(fast: bool = True) -> None:
+    """Compile the oracle libraries with the committed Makefile."""
+    targets = ["build/liboracle.so"] + (["build/liboracle_fast.so"] if fast else [])
+    subprocess.run(["make", "-s", "-C", _HERE] + targets, check=True)
+
+
+_libs: dict = {}
+
+
+def lib(fast: bool = False) -> C.CDLL:
+    name = "liboracle_fast.so" if fast else "liboracle.so"
+    if name not in _libs:
+        path = os.path.join(_BUILD, name)
+        if not os.path.exists(path):
+            build(fast=fast)
+        L = C.CDLL(path)
+        P, U32, U64, I32, F32, VP = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float, C.c_void_p
+        L.orc_dense_create.restype = P
+        L.orc_dense_create.argtypes = [P, U32, P, P, P, C.c_int, P, P, P, P, P]
+        L.orc_vdb_create.restype = P
+        L.orc_vdb_create.argtypes = [U64, P, P, P, U32, U32, P, P, P, P, P]
+        L.orc_destroy.argtypes = [P]
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_get_info.argtypes = [P, P, P, P, P, P, P]
+        L.orc_level_num_nodes.restype = U64
+        L.orc_level_num_nodes.argtypes = [P, U32]
+        L.orc_get_level.argtypes = [P, U32, P, P, P]
+        L.orc_value_range.argtypes = [P, U32, P]
+        L.orc_sample.argtypes = [P, C.c_int, U32, U64, P, U32, P]
+        L.orc_gradient.argtypes = [P, C.c_int, U32, U64, P, U32, P]
+        L.orc_sample_parallel.argtypes = [P, C.c_int, U64, P, U32, P, C.c_int]
+        L.orc_sample_fp64.argtypes = [P, C.c_int, U64, P, U32, P]
+        L.orc_iterate_intervals.argtypes = [P, U32, U32, P, F32, U64, P, P, P, U32, P, P]
+        L.orc_iterate_hits.argtypes = [P, U32, C.c_int, U32, P, U64, P, P, P, U32, P, P]
+        L.orc_tricubic_map.restype = C.c_int
+        L.orc_tricubic_map.argtypes = [P, P, P]
+        L.orc_inner_nodes.restype = U64
+        L.orc_inner_nodes.argtypes = [P, U32, U32, U64, P]
+        _libs[name] = L
+    return _libs[name]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OracleVolume:
+    """A committed oracle volume (dense structuredRegular or sparse VDB)."""
+
+    def __init__(self, handle, keep, fast=False):
+        self._h = handle
+        self._keep = keep  # numpy buffers the oracle points into
+        self._lib = lib(fast)
+        info = self.info()
+        self.dense = keep.get("dense", False)
+        self.o2i, self.i2o = info["o2i"], info["i2o"]
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.orc_destroy(self._h)
+        except Exception:
+            pass
+
+    # ---- construction -------------------------------------------------
+    @staticmethod
+    def dense_volume(data, cell_centered=False, grid_origin=None, grid_spacing=None,
+                     index_to_object=None, index_origin=None, background=None, fast=False):
+        """`data`: one array (or a list of arrays, one per attribute) shaped
+        (Z, Y, X) so that x is fastest in memory."""
+        arrays = data if isinstance(data, (list, tuple)) else [data]
+        arrays = [np.ascontiguousarray(a) for a in arrays]
+        dims = np.array(arrays[0].shape[::-1], np.int32)
+        ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+        types = np.array([_NP2VKL[a.dtype] for a in arrays], np.uint32)
+        strides = np.array([a.dtype.itemsize for a in arrays], np.uint64)
+        go = None if grid_origin is None else np.asarray(grid_origin, np.float32)
+        gs = None if grid_spacing is None else np.asarray(grid_spacing, np.float32)
+        i2o = None if index_to_object is None else np.asarray(index_to_object, np.float32)
+        io = None if index_origin is None else np.asarray(index_origin, np.int32)
+        bg = None if background is None else np.asarray(background, np.float32).reshape(-1)
+        L = lib(fast)
+        h = L.orc_dense_create(_p(dims), len(arrays), ptrs, _p(types), _p(strides),
+                               int(bool(cell_centered)), _p(go), _p(gs), _p(i2o), _p(io), _p(bg))
+        if not h:
+            raise RuntimeError(L.orc_last_error().decode())
+        return OracleVolume(h, {"arrays": arrays, "dense": True}, fast)
+
+    @staticmethod
+    def vdb_volume(levels, origins, formats, packed_dense, packed_tile=None,
+                   index_to_object=None, index_clipping_bounds=None, background=None, fast=False):
+        levels = np.ascontiguousarray(levels, np.uint32)
+        origins = np.ascontiguousarray(origins, np.int32).reshape(-1, 3)
+        formats = np.ascontiguousarray(formats, np.uint32)
+        pd = packed_dense if isinstance(packed_dense, (list, tuple)) else [packed_dense]
+        pd = [np.ascontiguousarray(a) for a in pd]
+        if packed_tile is None:
+            pt = [np.zeros(0, pd[0].dtype) for _ in pd]
+        else:
+            pt = packed_tile if isinstance(packed_tile, (list, tuple)) else [packed_tile]
+            pt = [np.ascontiguousarray(a) for a in pt]
+        dtype = _NP2VKL[pd[0].dtype]
+        pdp = (C.c_void_p * len(pd))(*[a.ctypes.data for a in pd])
+        ptp = (C.c_void_p * len(pt))(*[a.ctypes.data for a in pt])
+        i2o = None if index_to_object is None else np.asarray(index_to_object, np.float32)
+        clip = None if index_clipping_bounds is None else np.asarray(index_clipping_bounds, np.int32)
+        bg = None if background is None else np.asarray(background, np.float32).reshape(-1)
+        L = lib(fast)
+        h = L.orc_vdb_create(len(levels), _p(levels), _p(origins), _p(formats), len(pd), dtype,
+                             pdp, ptp, _p(i2o), _p(clip), _p(bg))
+        if not h:
+            raise RuntimeError(L.orc_last_error().decode())
+        return OracleVolume(h, {"pd": pd, "pt": pt, "dense": False}, fast)
+
+    # ---- introspection ------------------------------------------------
+    def info(self):
+        o2i = np.zeros(12, np.float32)
+        i2o = np.zeros(12, np.float32)
+        root = np.zeros(3, np.int32)
+        active = np.zeros(3, np.uint32)
+        dom = np.zeros(6, np.float32)
+        bounds = np.zeros(6, np.float32)
+        self._lib.orc_get_info(self._h, _p(o2i), _p(i2o), _p(root), _p(active), _p(dom), _p(bounds))
+        return dict(o2i=o2i, i2o=i2o, root=root, active=active, domain=dom, bounds=bounds)
+
+    def num_nodes(self, level):
+        return int(self._lib.orc_level_num_nodes(self._h, level))
+
+    def level(self, level, num_attributes=1):
+        n = self.num_nodes(level)
+        nv = n * (1 << (3 * [6, 5, 4, 3][level]))
+        vox = np.zeros(nv, np.uint64)
+        rng = np.zeros((nv * num_attributes, 2), np.float32)
+        org = np.zeros((n, 3), np.uint32)
+        self._lib.orc_get_level(self._h, level, _p(vox), _p(rng), _p(org))
+        return vox, rng, org
+
+    def value_range(self, attr=0):
+        r = np.zeros(2, np.float32)
+        self._lib.orc_value_range(self._h, attr, _p(r))
+        return r
+
+    # ---- sampling -----------------------------------------------------
+    def sample(self, points, filter=FILTER_LINEAR, attr=0, max_sampling_depth=3):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.float32)
+        self._lib.orc_sample(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out))
+        return out
+
+    def sample_parallel(self, points, filter=FILTER_LINEAR, attr=0, threads=0):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.float32)
+        self._lib.orc_sample_parallel(self._h, filter, len(pts), _p(pts), attr, _p(out), threads)
+        return out
+
+    def gradient(self, points, filter=FILTER_LINEAR, attr=0, max_sampling_depth=3):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros((len(pts), 3), np.float32)
+        self._lib.orc_gradient(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out))
+        return out
+
+    def sample_fp64(self, points, filter=FILTER_LINEAR, attr=0):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.float64)
+        self._lib.orc_sample_fp64(self._h, filter, len(pts), _p(pts), attr, _p(out))
+        return out
+
+    # ---- iteration ----------------------------------------------------
+    def intervals(self, origins, directions, t_ranges, value_ranges=None, hint=0.5, attr=0,
+                  max_intervals=64):
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(t_ranges, np.float32).reshape(-1, 2)
+        vr = None if value_ranges is None else np.ascontiguousarray(value_ranges, np.float32).reshape(-1, 2)
+        nvr = 0 if vr is None else len(vr)
+        out = np.zeros((len(o), max_intervals, 5), np.float32)
+        cnt = np.zeros(len(o), np.uint32)
+        self._lib.orc_iterate_intervals(self._h, attr, nvr, _p(vr), hint, len(o), _p(o), _p(d),
+                                        _p(t), max_intervals, _p(out), _p(cnt))
+        return out, cnt
+
+    def hits(self, origins, directions, t_ranges, values, filter=FILTER_LINEAR, attr=0, max_hits=16):
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(t_ranges, np.float32).reshape(-1, 2)
+        v = np.ascontiguousarray(values, np.float32).reshape(-1)
+        out = np.zeros((len(o), max_hits, 3), np.float32)
+        cnt = np.zeros(len(o), np.uint32)
+        self._lib.orc_iterate_hits(self._h, attr, filter, len(v), _p(v), len(o), _p(o), _p(d),
+                                   _p(t), max_hits, _p(out), _p(cnt))
+        return out, cnt
+
+    def inner_nodes(self, max_depth=1, attr=0):
+        n = int(self._lib.orc_inner_nodes(self._h, max_depth, attr, 0, None))
+        out = np.zeros((n, 8), np.float32)
+        self._lib.orc_inner_nodes(self._h, max_depth, attr, n, _p(out))
+        return out
+
+
+def tricubic_map():
+    """(start[65], cols[nnz], weights[nnz]) of the oracle's coefficient map."""
+    L = lib()
+    nnz = L.orc_tricubic_map(None, None, None)
+    start = np.zeros(65, np.int32)
+    cols = np.zeros(nnz, np.int32)
+    w = np.zeros(nnz, np.float32)
+    L.orc_tricubic_map(_p(start), _p(cols), _p(w))
+    return start, cols, w

@@ -1,0 +1,150 @@
+"""GPU parity of the cuda device's structuredRegular sampling and gradients
+against the oracle, through the C-ABI.
+
+The device arithmetic restates the reference's float expressions operation by
+operation, so results are compared bit for bit (uint32 patterns, NaN
+backgrounds included).  The same inputs are also scored against the FP64
+evaluation of the same filters (documented tolerance 1e-5 relative to the
+field's magnitude) to state the FP32 error.
+"""
+import numpy as np
+import pytest
+
+from openvkl_b200.fields import sinusoid_field, uniform_points
+from tests.conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+FILTERS = {"nearest": 0, "linear": 100, "cubic": 200}
+
+
+def _pts_around(dims, n, seed, pad=1.5):
+    lo = np.array([-pad] * 3)
+    hi = np.array(dims, np.float64) - 1 + pad
+    return uniform_points(n, lo, hi, seed)
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.uint16, np.float16, np.float32, np.float64])
+@pytest.mark.parametrize("filt", list(FILTERS))
+def test_dense_types_and_filters_bit_exact(vkl, device, oracle, dtype, filt):
+    dims = (21, 17, 13)  # not multiples of the 8^3 leaf
+    f = sinusoid_field(dims, seed=3)
+    if np.issubdtype(dtype, np.integer):
+        info = np.iinfo(dtype)
+        f = np.clip(f * 40 + (0 if info.min < 0 else 60), info.min, info.max)
+    vox = f.astype(dtype)
+    pts = _pts_around(dims, 20000, seed=4)
+    ref = oracle.OracleVolume.dense_volume(vox)
+    vol = vkl.structured_regular(device, vox)
+    smp = vkl.Sampler(vol, filter=FILTERS[filt], gradient_filter=FILTERS[filt])
+    s = smp.sample(pts)
+    np.testing.assert_array_equal(bits(s), bits(ref.sample(pts, filter=FILTERS[filt])))
+    g = smp.gradient(pts)
+    np.testing.assert_array_equal(bits(g), bits(ref.gradient(pts, filter=FILTERS[filt])))
+
+
+@pytest.mark.parametrize("cell", [False, True])
+def test_transform_background_and_origin(vkl, device, oracle, cell):
+    dims = (16, 24, 20)
+    vox = sinusoid_field(dims, seed=7)
+    ang = 0.3
+    c, s_ = np.cos(ang), np.sin(ang)
+    # column-major [vx vy vz p]: rotation about z, anisotropic scale, offset
+    i2o = np.array([0.5 * c, 0.5 * s_, 0, -0.7 * s_, 0.7 * c, 0, 0, 0, 0.25, 3.0, -2.0, 1.5], np.float32)
+    kw = dict(cell_centered=cell, index_to_object=i2o, index_origin=(-3, 5, 2), background=[0.125])
+    ref = oracle.OracleVolume.dense_volume(vox, **kw)
+    vol = vkl.structured_regular(device, vox, **kw)
+    np.testing.assert_array_equal(vol.bounding_box(), ref.info()["bounds"])
+    b = ref.info()["bounds"]
+    pts = uniform_points(30000, b[:3] - 0.5, b[3:] + 0.5, seed=9)
+    for name, fv in FILTERS.items():
+        smp = vkl.Sampler(vol, filter=fv, gradient_filter=fv)
+        np.testing.assert_array_equal(bits(smp.sample(pts)), bits(ref.sample(pts, filter=fv)), err_msg=name)
+        np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts, filter=fv)), err_msg=name)
+    np.testing.assert_array_equal(vol.value_range(), ref.value_range())
+
+
+def test_config1_full_size_linear_and_gradient(vkl, device, oracle):
+    """structuredRegular 128^3 float32 vertex-centered, seeded sinusoid field,
+    2^20 uniform points: vklComputeSampleN + vklComputeGradientN."""
+    dims = (128, 128, 128)
+    vox = sinusoid_field(dims, seed=1)
+    pts = uniform_points(1 << 20, (0, 0, 0), (127, 127, 127), seed=2)
+    ref = oracle.OracleVolume.dense_volume(vox)
+    vol = vkl.structured_regular(device, vox)
+    smp = vkl.Sampler(vol)
+    s = smp.sample(pts)
+    np.testing.assert_array_equal(bits(s), bits(ref.sample(pts)))
+    np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts)))
+    # error vs the FP64 evaluation of the same trilinear filter
+    d = ref.sample_fp64(pts[:100000])
+    rel = np.abs(s[:100000].astype(np.float64) - d) / np.maximum(np.abs(d), 1.0)
+    assert rel.max() < 1e-5
+
+
+def test_device_pointers_and_multi_attribute(vkl, device, oracle):
+    import torch
+    dims = (32, 32, 32)
+    a0 = sinusoid_field(dims, seed=1)
+    a1 = sinusoid_field(dims, seed=2).astype(np.float16)
+    a2 = (sinusoid_field(dims, seed=3) * 100).astype(np.int16)
+    ref = oracle.OracleVolume.dense_volume([a0, a1, a2])
+    vol = vkl.structured_regular(device, [a0, a1, a2])
+    assert vol.num_attributes() == 3
+    smp = vkl.Sampler(vol)
+    pts = _pts_around(dims, 5000, seed=5)
+    out = smp.sample_m(pts, [2, 0, 1])
+    for j, a in enumerate([2, 0, 1]):
+        np.testing.assert_array_equal(bits(out[:, j]), bits(ref.sample(pts, attr=a)))
+    # device-resident inputs / outputs are used in place
+    tp = torch.from_numpy(pts).cuda()
+    ts = smp.sample(tp, attr=1)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(bits(ts.cpu().numpy()), bits(ref.sample(pts, attr=1)))
+
+
+def test_scalar_and_wide_entry_points(vkl, device, oracle):
+    dims = (16, 16, 16)
+    vox = sinusoid_field(dims, seed=11)
+    ref = oracle.OracleVolume.dense_volume(vox)
+    vol = vkl.structured_regular(device, vox)
+    smp = vkl.Sampler(vol, filter=200, gradient_filter=200)
+    pts = _pts_around(dims, 16, seed=6, pad=-1.0)
+    want = ref.sample(pts, filter=200)
+    for i in range(4):
+        assert bits(np.float32(smp.sample_one(pts[i])))[()] == bits(want[i])[()]
+    np.testing.assert_array_equal(bits(smp.gradient_one(pts[0])), bits(ref.gradient(pts[:1], filter=200)[0]))
+    for w in (4, 8, 16):
+        valid = (np.arange(w) % 3 != 1).astype(np.int32)
+        got = smp.sample_w(pts[:w], valid=valid)
+        np.testing.assert_array_equal(bits(got[valid == 1]), bits(want[:w][valid == 1]))
+
+
+def test_shared_device_buffer_and_strided_host_data(vkl, device, oracle):
+    import torch
+    dims = (24, 16, 8)
+    vox = sinusoid_field(dims, seed=13)
+    ref = oracle.OracleVolume.dense_volume(vox)
+    tvox = torch.from_numpy(vox).cuda()
+    vol = vkl.structured_regular(device, tvox, shared=True)
+    pts = _pts_around(dims, 4000, seed=8)
+    np.testing.assert_array_equal(bits(vkl.Sampler(vol).sample(pts)), bits(ref.sample(pts)))
+    # strided host source: every other float of an interleaved buffer
+    inter = np.stack([vox, np.zeros_like(vox)], -1)
+    v2 = vkl.Volume(device, "structuredRegular")
+    v2.set_vec3i("dimensions", dims)
+    v2.set_data("data", vkl.Data(device, inter, vkl_type=vkl.VKL_FLOAT, num_items=vox.size, byte_stride=8))
+    v2.commit()
+    np.testing.assert_array_equal(bits(vkl.Sampler(v2).sample(pts)), bits(ref.sample(pts)))
+
+
+def test_error_paths(vkl, device):
+    v = vkl.Volume(device, "structuredRegular")
+    v.set_vec3i("dimensions", (4, 4, 4))
+    with pytest.raises(vkl.VKLError, match="missing required 'data'"):
+        v.commit()
+    v.set_data("data", vkl.Data(device, np.zeros(10, np.float32)))
+    with pytest.raises(vkl.VKLError, match="has 10 elements, but expected 64"):
+        v.commit()
+    with pytest.raises(vkl.VKLError):
+        vkl.Volume(device, "unstructured")

@@ -1,0 +1,112 @@
+"""GPU parity of the cuda device's VDB path against the oracle: tree
+construction (node / leaf indexing and per-voxel value ranges bit-exact),
+sparse sampling and gradients for all filters, FP16 leaves, tiles on upper
+levels, maxSamplingDepth, node.data input, and the dense tree."""
+import numpy as np
+import pytest
+
+from openvkl_b200.fields import shell_leaves, sinusoid_field, uniform_points
+from tests.conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+
+def _shell_vdb(domain=128, seed=5, dtype=np.float32, tiles=True):
+    origins, values = shell_leaves(domain=domain, shells=2, thickness=0.06, seed=seed)
+    L = len(origins)
+    levels = np.full(L, 3, np.uint32)
+    formats = np.ones(L, np.uint32)
+    tile_vals = np.zeros(0, np.float32)
+    if tiles:
+        # level-2 tiles (128^3) and level-1 tiles (4096^3) away from the leaves
+        t_orig = np.array([[domain + 4096, 0, 0], [0, domain + 128, 0], [8192, 8192, 8192]], np.int32)
+        t_lvl = np.array([2, 2, 1], np.uint32)
+        origins = np.concatenate([origins, t_orig])
+        levels = np.concatenate([levels, t_lvl])
+        formats = np.concatenate([formats, np.zeros(3, np.uint32)])
+        tile_vals = np.array([0.25, 0.75, 0.5], np.float32)
+    return origins, levels, formats, values.astype(dtype), tile_vals.astype(dtype)
+
+
+def _check_tree(vol, ref, num_attr=1):
+    for level in range(3):
+        vox, rng, org = vol.tree_level(level)
+        rvox, rrng, rorg = ref.level(level, num_attr)
+        assert len(org) == ref.num_nodes(level)
+        np.testing.assert_array_equal(vox, rvox)
+        np.testing.assert_array_equal(org, rorg)
+        np.testing.assert_array_equal(bits(rng), bits(rrng))
+    assert vol.tree_level(3) == ref.num_nodes(3)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float16])
+def test_sparse_tree_and_sampling_bit_exact(vkl, device, oracle, dtype):
+    origins, levels, formats, vals, tvals = _shell_vdb(dtype=dtype)
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tvals)
+    _check_tree(vol, ref)
+    np.testing.assert_array_equal(vol.bounding_box(), ref.info()["bounds"])
+    np.testing.assert_array_equal(vol.value_range(), ref.value_range())
+    rng = np.random.default_rng(3)
+    # points near active leaves and anywhere in the (large) domain
+    leaf_pts = (origins[:len(vals) // 512][rng.integers(0, len(vals) // 512, 30000)]
+                + rng.uniform(-2, 10, (30000, 3))).astype(np.float32)
+    b = ref.info()["bounds"]
+    far = uniform_points(10000, b[:3] - 4, b[3:] + 4, seed=4)
+    pts = np.concatenate([leaf_pts, far])
+    for fv in (0, 100, 200):
+        smp = vkl.Sampler(vol, filter=fv, gradient_filter=fv)
+        np.testing.assert_array_equal(bits(smp.sample(pts)), bits(ref.sample(pts, filter=fv)))
+        np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts, filter=fv)))
+
+
+@pytest.mark.parametrize("depth", [0, 1, 2])
+def test_max_sampling_depth(vkl, device, oracle, depth):
+    origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=9)
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tvals)
+    smp = vkl.Sampler(vol, max_sampling_depth=depth)
+    rng = np.random.default_rng(1)
+    pts = (origins[rng.integers(0, len(origins), 5000)] + rng.uniform(0, 8, (5000, 3))).astype(np.float32)
+    np.testing.assert_array_equal(bits(smp.sample(pts)),
+                                  bits(ref.sample(pts, max_sampling_depth=depth)))
+
+
+def test_node_data_input_matches_packed(vkl, device, oracle):
+    origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=2)
+    n_dense = len(vals) // 512
+    node_data = [vals[i * 512:(i + 1) * 512] for i in range(n_dense)] + [tvals[i:i + 1] for i in range(len(tvals))]
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = vkl.vdb_volume(device, levels, origins, formats, node_data=node_data)
+    rng = np.random.default_rng(7)
+    pts = (origins[rng.integers(0, len(origins), 8000)] + rng.uniform(-1, 9, (8000, 3))).astype(np.float32)
+    np.testing.assert_array_equal(bits(vkl.Sampler(vol).sample(pts)), bits(ref.sample(pts)))
+
+
+def test_dense_tree_bit_exact(vkl, device, oracle):
+    dims = (300, 140, 36)  # several level-2 nodes, partial leaves
+    vox = sinusoid_field(dims, seed=5)
+    ref = oracle.OracleVolume.dense_volume(vox, background=[-2.0])
+    vol = vkl.structured_regular(device, vox, background=[-2.0])
+    _check_tree(vol, ref)
+    np.testing.assert_array_equal(vol.value_range(), ref.value_range())
+
+
+def test_inner_node_observer_matches_oracle(vkl, device, oracle):
+    origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=4)
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tvals)
+    for depth in (0, 1, 2):
+        got = vol.inner_nodes(max_depth=depth)
+        want = ref.inner_nodes(max_depth=depth)
+        key = lambda a: a[np.lexsort(a.T[::-1])]
+        np.testing.assert_array_equal(key(got), key(want))
+
+
+def test_vdb_validation_errors(vkl, device):
+    data = np.zeros(512, np.float32)
+    with pytest.raises(vkl.VKLError) as e:
+        vkl.vdb_volume(device, [4], [[0, 0, 0]], [1], node_data=[data])
+    assert e.value.code == 1 and e.value.msg == "invalid node level 4 for this vdb configuration"
+    with pytest.raises(vkl.VKLError, match="Node data too small"):
+        vkl.vdb_volume(device, [3], [[0, 0, 0]], [1], node_data=[data[:1]])
