@@ -1,0 +1,426 @@
+"""Benchmark of the cuda device's hot path on B200.
+
+Workload (default, "coherent"): structuredRegular 1024^3 float32
+vertex-centered volume (seeded sum of 4 sinusoids + noise), trilinear
+vklComputeSampleN over 1920x1080 orbit-camera rays x 256 jittered samples
+each = 530,841,600 points per step.  Other workloads: "incoherent" (2^26
+uniform random points, same volume), "cubic" (coherent points, tricubic
+filter), "gradient" (coherent points, trilinear gradients).
+
+One JSON line (rank 0):
+  value       Gsamples/s over all ranks, device-timed with CUDA events on the
+              launching stream over exactly --steps steps (inputs resident in
+              HBM; inputs are larger than L2, so no flush is needed)
+  e2e         the same metric through the C API with pinned host buffers:
+              H2D of the points, kernel, D2H of the samples, every step
+  roofline    dominant kernel's algorithmic bytes per launch / launch time
+              against the measured HBM copy bandwidth
+  cpu_baseline the oracle (C++ restatement of the reference CPU device)
+              on all host cores, on a bounded sample of the same workload
+
+--impl reference times that CPU implementation alone (rank 0) and prints its
+line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (1024, 1024, 1024)
+WIDTH, HEIGHT, SPP = 1920, 1080, 256
+INCOHERENT_N = 1 << 26
+METRIC = "Gsamples/s and HBM GB/s (% roofline): plain FP32 vs FP16/FP8/batched/MLP at stated error"
+UNIT = "Gsamples/s"
+MAX_CPU_POINTS = 1 << 27  # bounded CPU sample (1.6 GB of points)
+FILTER = {"coherent": 100, "incoherent": 100, "cubic": 200, "gradient": 100}
+
+
+# ---------------------------------------------------------------------------
+# Workload generation.
+# ---------------------------------------------------------------------------
+def volume_numpy(dims=None, seed=1):
+    """Seeded sinusoid field, generated slab by slab in float32 (x fastest)."""
+    from openvkl_b200.fields import _sinusoid_params
+    X, Y, Z = dims or DIMS
+    freq, amp, phase = _sinusoid_params(seed)
+    rng = np.random.default_rng(seed + 1000)
+    out = np.empty((Z, Y, X), np.float32)
+    x = (np.arange(X, dtype=np.float32) / X)[None, :]
+    y = (np.arange(Y, dtype=np.float32) / Y)[:, None]
+    two_pi = np.float32(2 * math.pi)
+    # sin(a + c) with a = 2pi(fx x + fy y) + phase per term, c = 2pi fz z
+    sa, ca = [], []
+    for k in range(4):
+        a = two_pi * (np.float32(freq[k, 0]) * x + np.float32(freq[k, 1]) * y) + np.float32(phase[k])
+        sa.append(np.sin(a).astype(np.float32))
+        ca.append(np.cos(a).astype(np.float32))
+    for zi in range(Z):
+        acc = rng.uniform(-0.05, 0.05, size=(Y, X)).astype(np.float32)
+        for k in range(4):
+            c = 2 * math.pi * freq[k, 2] * zi / Z
+            acc += np.float32(amp[k]) * (sa[k] * np.float32(math.cos(c)) + ca[k] * np.float32(math.sin(c)))
+        out[zi] = acc
+    return out
+
+
+def points_torch(workload, dims=None, device="cuda"):
+    from openvkl_b200 import fields
+    hi = tuple(d - 1 for d in (dims or DIMS))
+    if workload == "incoherent":
+        return fields.uniform_points_torch(INCOHERENT_N, (0, 0, 0), hi, seed=2, device=device)
+    return fields.orbit_camera_samples_torch(WIDTH, HEIGHT, SPP, (0, 0, 0), hi, seed=3, device=device)
+
+
+def points_numpy_sample(workload, n_rays_or_pts, dims=None):
+    """A bounded sample of the same workload generated on the host."""
+    from openvkl_b200 import fields
+    hi = tuple(d - 1 for d in (dims or DIMS))
+    if workload == "incoherent":
+        return fields.uniform_points(n_rays_or_pts, (0, 0, 0), hi, seed=2)
+    # the first rows of the image: whole rays, ray-major like the full set
+    rows = max(1, n_rays_or_pts // WIDTH)
+    full_h = HEIGHT
+    pts = fields.orbit_camera_samples(WIDTH, full_h, SPP, (0, 0, 0), hi, seed=3) if rows >= full_h else \
+        _camera_rows(rows, hi)
+    return pts
+
+
+def _camera_rows(rows, hi):
+    """Samples of the first `rows` image rows of the orbit camera."""
+    from openvkl_b200 import fields
+    eye, fwd, right, up, sx, sy = fields._camera_rays(WIDTH, HEIGHT, (0, 0, 0), hi, 0.7)
+    rng = np.random.default_rng(3)
+    u = (np.arange(WIDTH) + 0.5) / WIDTH * 2 - 1
+    v = ((np.arange(rows) + 0.5) / HEIGHT * 2 - 1)
+    uu, vv = np.meshgrid(u, v)
+    d = fwd[None, :] + uu.reshape(-1, 1) * sx * right[None, :] + vv.reshape(-1, 1) * sy * up[None, :]
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t0, t1 = fields._slab(eye, d, np.zeros(3), np.asarray(hi, np.float64))
+    j = (np.arange(SPP)[None, :] + rng.random((d.shape[0], SPP))) / SPP
+    t = t0[:, None] + j * (t1 - t0)[:, None]
+    return (eye[None, None, :] + t[:, :, None] * d[:, None, :]).reshape(-1, 3).astype(np.float32)
+
+
+def compulsory_bytes(points, dims, filter_):
+    """Unique 32-byte sectors of the volume touched by all stencils x 32."""
+    import torch
+    X, Y, Z = dims
+    nsect = (X * Y * Z * 4 + 31) // 32
+    mark = torch.zeros(nsect, dtype=torch.bool, device=points.device)
+    lo, hi = (0, 2) if filter_ != 200 else (-1, 3)
+    chunk = 1 << 22
+    for s in range(0, points.shape[0], chunk):
+        p = points[s:s + chunk]
+        ic = torch.floor(p).to(torch.int64)
+        for dz in range(lo, hi):
+            for dy in range(lo, hi):
+                for dx in range(lo, hi):
+                    x, y, z = ic[:, 0] + dx, ic[:, 1] + dy, ic[:, 2] + dz
+                    ok = (x >= 0) & (x < X) & (y >= 0) & (y < Y) & (z >= 0) & (z < Z)
+                    e = ((z * Y + y) * X + x)[ok]
+                    mark[(e * 4) // 32] = True
+    return int(mark.sum().item()) * 32
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle restatement of the reference CPU device).
+# ---------------------------------------------------------------------------
+def cpu_baseline(vox, workload, budget_s=15.0):
+    """Times the oracle on all host threads on a bounded sample sized for
+    about `budget_s` seconds of work."""
+    from oracle import pyoracle as O
+    threads = os.cpu_count() or 1
+    f = FILTER[workload]
+    v = O.OracleVolume.dense_volume(vox, fast=True)
+    L = O.lib(True)
+
+    def run(pts):
+        out = np.empty(len(pts), np.float32)
+        t = time.perf_counter()
+        if workload == "gradient":
+            g = np.empty((len(pts), 3), np.float32)
+            L.orc_gradient(v._h, f, 3, len(pts), pts.ctypes.data, 0, g.ctypes.data)
+        else:
+            L.orc_sample_parallel(v._h, f, len(pts), pts.ctypes.data, 0, out.ctypes.data, threads)
+        return time.perf_counter() - t
+
+    probe = points_numpy_sample(workload, WIDTH * 8 if workload != "incoherent" else 1 << 20)
+    dt = run(probe)
+    rate = len(probe) / max(dt, 1e-6)
+    n = int(min(rate * budget_s, MAX_CPU_POINTS))
+    n = max(n, len(probe))
+    pts = points_numpy_sample(workload, n if workload == "incoherent" else max(1, n // SPP))
+    reps = max(1, int(budget_s * rate / len(pts)))
+    t = time.perf_counter()
+    for _ in range(reps):
+        run(pts)
+    dt = time.perf_counter() - t
+    cores = 1 if workload == "gradient" else threads
+    what = "first image rows" if workload != "incoherent" else "same seed"
+    return {"value": reps * len(pts) / dt / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(pts)} points of the same workload ({what}) x {reps} passes; oracle C++ "
+                      f"restatement of the reference CPU device, -O3 -march=native, {cores} host "
+                      f"threads, {dt:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# Runs.
+# ---------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    vox = volume_numpy()
+    from oracle import pyoracle as O
+    threads = os.cpu_count() or 1
+    f = FILTER[args.workload]
+    v = O.OracleVolume.dense_volume(vox, fast=True)
+    L = O.lib(True)
+    # size each step so the whole run stays within a few minutes
+    probe = points_numpy_sample(args.workload, WIDTH * 4 if args.workload != "incoherent" else 1 << 20)
+    out = np.empty(len(probe), np.float32)
+    t = time.perf_counter()
+    L.orc_sample_parallel(v._h, f, len(probe), probe.ctypes.data, 0, out.ctypes.data, threads)
+    rate = len(probe) / max(time.perf_counter() - t, 1e-6)
+    per_step_s = min(10.0, 120.0 / max(1, args.steps + args.warmup))
+    n = max(len(probe), min(MAX_CPU_POINTS, int(rate * per_step_s)))
+    pts = points_numpy_sample(args.workload, n if args.workload == "incoherent" else max(1, n // SPP))
+    out = np.empty(len(pts), np.float32)
+    for _ in range(args.warmup):
+        L.orc_sample_parallel(v._h, f, len(pts), pts.ctypes.data, 0, out.ctypes.data, threads)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        L.orc_sample_parallel(v._h, f, len(pts), pts.ctypes.data, 0, out.ctypes.data, threads)
+    dt = (time.perf_counter() - t) / args.steps
+    value = len(pts) / dt / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_of(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(pts)} points of the same workload per step; oracle C++ restatement "
+                                   f"of the reference CPU device (the ISPC device cannot be built here), "
+                                   f"-O3 -march=native, {threads} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args):
+    n = INCOHERENT_N if args.workload == "incoherent" else WIDTH * HEIGHT * SPP
+    return {"workload": f"structuredRegular 1024^3 float32 vertex-centered, "
+                        f"{'tricubic' if args.workload == 'cubic' else 'trilinear'} "
+                        f"{'gradient' if args.workload == 'gradient' else 'sample'}N, "
+                        + ("1920x1080 orbit-camera rays x 256 jittered samples" if args.workload != "incoherent"
+                           else "2^26 uniform random points"),
+            "points_per_step": n, "volume_bytes": DIMS[0] * DIMS[1] * DIMS[2] * 4,
+            "l2": "inputs larger than L2 (4 GiB volume, >=805 MB points), no flush"}
+
+
+def run_cuda(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from openvkl_b200 import vkl
+
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vox = volume_numpy()
+    tvox = torch.from_numpy(vox).cuda()
+    vol = vkl.structured_regular(dev, tvox, shared=True)
+    f = FILTER[args.workload]
+    smp = vkl.Sampler(vol, filter=f, gradient_filter=f)
+    pts = points_torch(args.workload)
+    n = pts.shape[0]
+    grad = args.workload == "gradient"
+    out = torch.empty((n, 3) if grad else (n,), dtype=torch.float32, device="cuda")
+    call = smp.gradient if grad else smp.sample
+
+    for _ in range(args.warmup):
+        call(pts, out=out)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)  # let the sampler start
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            call(pts, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    value = n * ws / (ms * 1e-3) / 1e9
+
+    # algorithmic bytes of one launch: point in + result out + compulsory voxels
+    io = n * (12 + (12 if grad else 4))
+    comp = 0 if args.no_extras else compulsory_bytes(pts, DIMS, f)
+    alg = io + comp
+    peak, peak_kind = peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+
+    # end to end through the C API with pinned host buffers: every step copies
+    # the points host->device and the samples device->host (library staging)
+    e2e = None
+    if not args.no_extras:
+        hp = pts.cpu().pin_memory()
+        ho = torch.empty(out.shape, dtype=torch.float32).pin_memory()
+        call(hp, out=ho)  # first call sizes the staging buffers
+        e2e_steps = max(1, min(args.steps, 5))
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            call(hp, out=ho)
+        e2e_s = (time.perf_counter() - t) / e2e_steps
+        if ws > 1:
+            tt = torch.tensor([e2e_s], device="cuda")
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": n * ws / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 12,
+               "d2h_bytes_per_step": int(ho.numel()) * 4}
+        del hp, ho
+
+    line = None
+    if rank == 0:
+        clocks = clk.summary()
+        base = None if args.no_cpu_baseline else cpu_baseline(vox, args.workload)
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            tr = json.load(open(tp)).get(args.workload)
+            if tr:
+                traffic = tr["bytes_per_point"] * n
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sinusoid volume, generated rays)",
+            "config": config_of(args),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg, "compulsory_voxel_bytes": comp},
+            "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--workload", choices=list(FILTER), default="coherent")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="timed loop only (no e2e / roofline bytes / CPU baseline): profiling runs")
+    ap.add_argument("--small", action="store_true",
+                    help="512^3 volume, 480x270 rays x 256: the ncu capture case")
+    args = ap.parse_args(argv)
+    if args.small:
+        global DIMS, WIDTH, HEIGHT, INCOHERENT_N
+        DIMS, WIDTH, HEIGHT, INCOHERENT_N = (512, 512, 512), 480, 270, 1 << 24
+    if args.no_extras:
+        args.no_cpu_baseline = True
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -135,25 +135,17 @@ __device__ inline void queryVoxelDense(const DevGrid &g, int32_t x, int32_t y, i
     desc.isEmpty = true;
     return;
   }
-  const uint64_t nx1 = (g.activeSize[0] + levelRes(1) - 1) >> totalLogRes(1);
-  const uint64_t ny1 = (g.activeSize[1] + levelRes(1) - 1) >> totalLogRes(1);
-  const uint64_t l1  = (uint64_t)(oz >> totalLogRes(1)) * ny1 * nx1 +
-                      (uint64_t)(oy >> totalLogRes(1)) * nx1 + (uint64_t)(ox >> totalLogRes(1));
-  uint32_t lvl;
-  uint64_t ni;
-  if (depth >= 2) {
-    const uint64_t nx2 = (g.activeSize[0] + levelRes(2) - 1) >> totalLogRes(2);
-    const uint64_t ny2 = (g.activeSize[1] + levelRes(2) - 1) >> totalLogRes(2);
-    const uint64_t l2  = (uint64_t)(oz >> totalLogRes(2)) * ny2 * nx2 +
-                        (uint64_t)(oy >> totalLogRes(2)) * nx2 + (uint64_t)(ox >> totalLogRes(2));
-    ni  = l1 * levelNumVoxels(1) + l2 * levelNumVoxels(2) + offsetToLinear(2, ox, oy, oz);
-    lvl = 2;
-  } else if (depth == 1) {
-    ni  = l1 * levelNumVoxels(1) + offsetToLinear(1, ox, oy, oz);
-    lvl = 1;
-  } else {
-    ni  = offsetToLinear(0, ox, oy, oz);
-    lvl = 0;
+  // The reference computes the level-1/2 node numbers in closed form
+  // (z-major over the dense node grid, VdbQueryVoxelDense.ih:41-113); walking
+  // the child pointers gives the same voxel for every volume up to 4096^3
+  // and never indexes past a level's arrays beyond that.
+  const uint32_t lvl = depth >= 2 ? 2u : depth;
+  uint64_t node = 0, ni = 0;
+  for (uint32_t l = 0;; ++l) {
+    ni = node * levelNumVoxels(l) + offsetToLinear(l, ox, oy, oz);
+    if (l == lvl)
+      break;
+    node = voxelChildIndex(__ldg(g.levels[l].voxels + ni));
   }
   const float *r = g.levels[lvl].valueRange + 2 * (ni * g.numAttributes + attr);
   desc.v0        = __ldg(r);
@@ -217,9 +209,19 @@ __device__ inline void hddaStep(const VoxelDesc &desc, Dda &d)
   }
 }
 
+// Loop bounds.  The reference's loops end only when float t passes tMax;
+// on a GPU a ray whose t stops advancing (t + tDelta == t at huge t, or a
+// march step below t's ulp) must not spin forever, so every ray carries a
+// step budget; a ray that exhausts it ends its iteration as if it had left
+// the volume.  The oracle applies the same bounds, so results still match.
+constexpr uint32_t kMaxDdaSteps   = 1u << 26;  // hierarchical DDA steps per ray
+constexpr uint32_t kMaxMarchSteps = 1u << 24;  // bisection march steps per interval
+constexpr uint32_t kMaxHitsPerRay = 1u << 24;
+
 struct IntervalIt {
   float tMax;
   float nominalDeltaT;
+  uint32_t budget;
   Dda dda;
 };
 
@@ -252,6 +254,7 @@ __device__ inline void intervalInit(const DevGrid &g, uint32_t depth, f3 origin,
                           1.f * divideSafe(fabsf(dir.z)));
   float lo, hi;
   intersectBox(org, dir, g.domain, tLo, tHi, lo, hi);
+  it.budget = kMaxDdaSteps;
   if (hi <= lo) {
     it.tMax  = -kPosInf;
     it.dda.t = 0.f;
@@ -275,12 +278,20 @@ __device__ inline bool intervalNext(const DevGrid &g, uint32_t attr, const DevVa
       queryVoxelSparse(g, it.dda.idx[L], it.dda.idx[4 + L], it.dda.idx[8 + L], L, attr, vr, desc);
     if (!desc.isEmpty)
       break;
+    if (it.budget-- == 0) {
+      it.tMax = -kPosInf;
+      return false;
+    }
     hddaStep(desc, it.dda);
   }
   if (it.dda.t < it.tMax) {
     out.v0 = desc.v0;
     out.v1 = desc.v1;
     out.t0 = it.dda.t;
+    if (it.budget-- == 0) {
+      it.tMax = -kPosInf;
+      return false;
+    }
     hddaStep(desc, it.dda);
     out.t1            = minx(it.dda.t, it.tMax);
     out.nominalDeltaT = it.nominalDeltaT;
@@ -348,7 +359,7 @@ __device__ inline bool intersectBisection(const HitCtx &c, float tLo, float tHi,
     t0 += maxx(1e-5f, 1e-5f * step);
     s0 = c.sampleAt(t0);
   }
-  while (t0 < tHi) {
+  for (uint32_t march = 0; t0 < tHi && march < kMaxMarchSteps; ++march) {
     const float h = minx(step, tHi - t0);
     const float t = t0 + h;
     float s       = c.sampleAt(t);

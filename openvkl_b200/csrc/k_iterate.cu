@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid 
   hitInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), h);
   uint32_t c = 0;
   DevHit hit;
-  while (hitNext(g, filter, attr, kNumLevels - 1, vr, numValues, values, h, hit)) {
+  while (c < kMaxHitsPerRay && hitNext(g, filter, attr, kNumLevels - 1, vr, numValues, values, h, hit)) {
     if (c < maxPerRay)
       out[r * maxPerRay + c] = hit;
     ++c;

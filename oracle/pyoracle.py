@@ -29,19 +29,38 @@ _NP2VKL = {
 BACKGROUND_UNDEFINED = np.frombuffer(np.uint32(0xFFC068B5).tobytes(), np.float32)[0]
 
 
+def _host_tag() -> str:
+    """Short hash of this host's CPU model and ISA flags: the timing build is
+    compiled with -march=native, so each host gets its own copy."""
+    import hashlib
+    try:
+        info = open("/proc/cpuinfo").read()
+        model = [l for l in info.splitlines() if l.startswith(("model name", "flags"))][:2]
+    except OSError:
+        model = ["unknown"]
+    return hashlib.md5("\n".join(model).encode()).hexdigest()[:10]
+
+
+def fast_path() -> str:
+    return os.path.join(_BUILD, f"liboracle_fast_{_host_tag()}.so")
+
+
 def build(fast: bool = True) -> None:
-    """Compile the oracle libraries with the committed Makefile."""
-    targets = ["build/liboracle.so"] + (["build/liboracle_fast.so"] if fast else [])
-    subprocess.run(["make", "-s", "-C", _HERE] + targets, check=True)
+    """Compile the parity build with the committed Makefile and, if asked,
+    the -march=native timing build for this host."""
+    subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle.so"], check=True)
+    if fast and not os.path.exists(fast_path()):
+        subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle_fast.so"], check=True)
+        os.replace(os.path.join(_BUILD, "liboracle_fast.so"), fast_path())
 
 
 _libs: dict = {}
 
 
 def lib(fast: bool = False) -> C.CDLL:
-    name = "liboracle_fast.so" if fast else "liboracle.so"
+    name = fast_path() if fast else os.path.join(_BUILD, "liboracle.so")
     if name not in _libs:
-        path = os.path.join(_BUILD, name)
+        path = name
         if not os.path.exists(path):
             build(fast=fast)
         L = C.CDLL(path)

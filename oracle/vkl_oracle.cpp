@@ -1087,11 +1087,19 @@ static bool hddaStepL(uint32_t L, const VoxelDesc &desc, Dda &d)
   return stepped;
 }
 
+// Per-ray loop bounds shared with the CUDA device (a ray whose float t
+// stops advancing ends instead of spinning): DDA steps per ray, march steps
+// per bisection interval, hits per ray.
+constexpr uint32_t MAX_DDA_STEPS   = 1u << 26;
+constexpr uint32_t MAX_MARCH_STEPS = 1u << 24;
+constexpr uint32_t MAX_HITS        = 1u << 24;
+
 struct IntervalIt {
   const Grid *g;
   uint32_t attr;
   float tMax;
   float nominalDeltaT;
+  uint32_t budget;
   Dda dda;
 };
 
@@ -1134,6 +1142,7 @@ static void intervalInit(IntervalIt &it, const Grid &g, uint32_t attr, uint32_t 
   it.nominalDeltaT = fmin_(fmin_(1.f * rcp_safe(std::fabs(dir.x)), 1.f * rcp_safe(std::fabs(dir.y))),
                            1.f * rcp_safe(std::fabs(dir.z)));
   const range1f ti = intersectBox(org, dir, g.domain, tRange);
+  it.budget        = MAX_DDA_STEPS;
   if (ti.upper <= ti.lower) {
     it.tMax  = -std::numeric_limits<float>::infinity();
     it.dda.t = 0;
@@ -1160,11 +1169,19 @@ static bool intervalIterate(IntervalIt &it, const ValueRanges &vr, Interval &out
                        it.attr, vr, desc);
     if (!desc.isEmpty)
       break;
+    if (it.budget-- == 0) {
+      it.tMax = -std::numeric_limits<float>::infinity();
+      return false;
+    }
     hddaStepL(0, desc, it.dda);
   }
   if (it.dda.t < it.tMax) {
     out.v       = desc.valueRange;
     out.t.lower = it.dda.t;
+    if (it.budget-- == 0) {
+      it.tMax = -std::numeric_limits<float>::infinity();
+      return false;
+    }
     hddaStepL(0, desc, it.dda);
     out.t.upper       = fmin_(it.dda.t, it.tMax);
     out.nominalDeltaT = it.nominalDeltaT;
@@ -1248,7 +1265,7 @@ static bool intersectBisection(const Grid &g, int filter, uint32_t a, const vec3
     }
   }
   float t;
-  while (t0 < tr.upper) {
+  for (uint32_t march = 0; t0 < tr.upper && march < MAX_MARCH_STEPS; ++march) {
     const float h = fmin_(step, tr.upper - t0);
     t             = t0 + h;
     float sample  = S(t);
@@ -1687,7 +1704,7 @@ void orc_iterate_hits(const OrcVolume *v, uint32_t attr, int filter, uint32_t nu
       counts[r] = 0;
       return;
     }
-    while (true) {
+    while (c < MAX_HITS) {
       // one vklIterateHit call
       if (cur.t.lower == inf)
         break;

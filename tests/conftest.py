@@ -39,5 +39,11 @@ def device(vkl):
 
 
 def bits(a):
-    """float32 array -> uint32 bit patterns (NaN payloads compared exactly)."""
-    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+    """float32 array -> uint32 bit patterns for bit-exact comparison.
+
+    Every NaN maps to one pattern: arithmetic on a NaN background returns the
+    canonical NaN on the GPU but keeps the operand's payload on x86, and
+    both mean "undefined"; all non-NaN values compare bit for bit."""
+    a = np.array(a, np.float32, copy=True)
+    a[np.isnan(a)] = np.float32(np.nan)
+    return a.view(np.uint32)
