@@ -80,6 +80,18 @@ VKL_HD uint64_t offsetToLinear(uint32_t l, uint64_t x, uint64_t y, uint64_t z)
          ((z & mask) >> sh);
 }
 
+// Bricked dense layout: 8^3-voxel bricks (x fastest inside a brick), 8^3
+// bricks per 64^3 supertile (x fastest), supertiles x fastest.  A trilinear
+// stencil then touches one or two 2 KB bricks and a warp's rays stay within
+// a few MB, where the x-fastest layout puts every z step 4 MB apart (1024^2
+// floats) and thrashes the TLB and L2.
+VKL_HD uint64_t brickIndex(uint32_t x, uint32_t y, uint32_t z, uint32_t superX, uint32_t superY)
+{
+  const uint32_t st = ((z >> 6) * superY + (y >> 6)) * superX + (x >> 6);
+  const uint32_t b  = (((z >> 3) & 7u) << 6) | (((y >> 3) & 7u) << 3) | ((x >> 3) & 7u);
+  return ((uint64_t)st << 18) | ((uint64_t)b << 9) | ((z & 7u) << 6) | ((y & 7u) << 3) | (x & 7u);
+}
+
 struct DevLevel {
   uint64_t numNodes;
   const uint32_t *origin;  // 3 per node, root-relative
@@ -106,6 +118,9 @@ struct DevGrid {
   uint32_t constantCellData;
   uint32_t numAttributes;
   int32_t denseDims[3];
+  // Dense voxels are stored bricked (see brickIndex): the number of 64^3
+  // supertiles along x and y.
+  uint32_t superX, superY;
   DevLevel levels[kNumLevels - 1];
   uint64_t numLeaves;
   // Dense: attribute voxel arrays (x fastest).  Sparse: packed dense leaves

@@ -111,14 +111,12 @@ __global__ void __launch_bounds__(256) kDenseLeafRanges(const __grid_constant__ 
   const T *data = (const T *)g.data[attr];
   float lo = kInf, hi = -kInf;
   for (int32_t z = z0; z < z1; ++z)
-    for (int32_t y = y0; y < y1; ++y) {
-      const T *row = data + ((uint64_t)z * Y + y) * (uint64_t)X;
+    for (int32_t y = y0; y < y1; ++y)
       for (int32_t x = x0; x < x1; ++x) {
-        const float v = ldv(row, x);
+        const float v = ldv(data, brickIndex(x, y, z, g.superX, g.superY));
         lo            = fminx(lo, v);
         hi            = fmaxx(hi, v);
       }
-    }
   const bool boundary = ox - 8 < 0 || oy - 8 < 0 || oz - 8 < 0 || ox + 8 >= X || oy + 8 >= Y ||
                         oz + 8 >= Z;
   const float bg = g.background[attr];
@@ -297,6 +295,21 @@ __global__ void __launch_bounds__(1024) kVolumeRange(const __grid_constant__ Dev
 
 inline unsigned blocksFor(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
+// x-fastest user array -> bricked copy; one thread per voxel, element size
+// only (the layout does not depend on the voxel type).
+template <typename E>
+__global__ void kToBricked(const E *__restrict__ src, E *__restrict__ dst, uint3 dims, uint32_t superX,
+                           uint32_t superY)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t n = (uint64_t)dims.x * dims.y * dims.z;
+  if (i >= n)
+    return;
+  const uint32_t x = (uint32_t)(i % dims.x), y = (uint32_t)((i / dims.x) % dims.y),
+                 z = (uint32_t)(i / ((uint64_t)dims.x * dims.y));
+  dst[brickIndex(x, y, z, superX, superY)] = src[i];
+}
+
 }  // namespace
 
 void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint64_t *vox2,
@@ -370,6 +383,40 @@ void launchPropagateRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
       kReduceNodes<<<(unsigned)g.levels[l].numNodes, 256, 0, st>>>(g, attr, l);
   kVolumeRange<<<1, 1024, 0, st>>>(g, attr, volumeRange);
   cudaCheck(cudaGetLastError(), "range propagation kernels");
+}
+
+}  // namespace vklcuda
+
+namespace vklcuda {
+
+uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY)
+{
+  superX = (dims[0] + 63) / 64;
+  superY = (dims[1] + 63) / 64;
+  const uint64_t superZ = (dims[2] + 63) / 64;
+  return (uint64_t)superX * superY * superZ << 18;
+}
+
+void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
+                     uint32_t superX, uint32_t superY, cudaStream_t st)
+{
+  const uint3 D = {dims[0], dims[1], dims[2]};
+  const uint64_t n = (uint64_t)dims[0] * dims[1] * dims[2];
+  const unsigned grid = blocksFor(n, 256);
+  switch (elemBytes) {
+  case 1:
+    kToBricked<uint8_t><<<grid, 256, 0, st>>>((const uint8_t *)src, (uint8_t *)dst, D, superX, superY);
+    break;
+  case 2:
+    kToBricked<uint16_t><<<grid, 256, 0, st>>>((const uint16_t *)src, (uint16_t *)dst, D, superX, superY);
+    break;
+  case 4:
+    kToBricked<uint32_t><<<grid, 256, 0, st>>>((const uint32_t *)src, (uint32_t *)dst, D, superX, superY);
+    break;
+  default:
+    kToBricked<uint64_t><<<grid, 256, 0, st>>>((const uint64_t *)src, (uint64_t *)dst, D, superX, superY);
+  }
+  cudaCheck(cudaGetLastError(), "bricking kernel");
 }
 
 }  // namespace vklcuda

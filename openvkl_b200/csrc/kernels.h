@@ -18,6 +18,12 @@ void launchSample(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
 void launchGradient(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
                     const float *points, uint32_t attr, float *out, cudaStream_t stream);
 
+// Bricked copy of a dense x-fastest voxel array (brickIndex, grid.h):
+// returns the element count of the bricked array and its supertile counts.
+uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY);
+void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
+                     uint32_t superX, uint32_t superY, cudaStream_t stream);
+
 // Commit-time tree construction for dense volumes: fills the voxel codes and
 // node origins of levels 0..2 (closed form of the reference's insertion
 // order for x-fastest leaves).

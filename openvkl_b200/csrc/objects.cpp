@@ -402,10 +402,20 @@ void Volume::commitDense()
     std::memcpy(c, cc, sizeof(c));
   }
   makeTransforms(c, grid.indexToObject, grid.objectToIndex);
-  for (uint32_t a = 0; a < grid.numAttributes; ++a) {
-    keep.emplace_back(attrs[a]);
-    grid.data[a] = attrs[a]->dev;
-    grid.type[a] = attrs[a]->type;
+  // Each attribute is re-laid out once into the bricked order the kernels
+  // read (grid.h brickIndex); the padding of partial supertiles is zeroed
+  // and never read (every tap is checked against the domain first).
+  {
+    const uint32_t udims[3] = {(uint32_t)dims[0], (uint32_t)dims[1], (uint32_t)dims[2]};
+    const uint64_t nb = brickedElements(udims, grid.superX, grid.superY);
+    for (uint32_t a = 0; a < grid.numAttributes; ++a) {
+      const size_t es  = sizeOfType(attrs[a]->type);
+      DeviceBuffer *bb = newBuffer(nb * es);
+      cudaCheck(cudaMemsetAsync(bb->ptr, 0, nb * es, device->stream), "memset");
+      launchToBricked(attrs[a]->dev, bb->ptr, es, udims, grid.superX, grid.superY, device->stream);
+      grid.data[a] = bb->ptr;
+      grid.type[a] = attrs[a]->type;
+    }
   }
   // background: one value, or one per attribute (ManagedObject.h:59-66)
   {

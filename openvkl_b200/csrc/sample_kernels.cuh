@@ -5,6 +5,8 @@
 // VdbSampler.ispc:97-129 / :303-335, restated as template instantiation).
 // Each filter is instantiated in its own translation unit (k_sample_*.cu).
 #pragma once
+#include <type_traits>
+
 #include "kernels.h"
 #include "objects.h"
 #include "sampling.cuh"
@@ -28,62 +30,161 @@ __device__ __forceinline__ float filterAt(const Field &F, bool cc, f3 p)
   return sampleLinear(F, p);
 }
 
-template <typename T, bool DENSE, int FILTER>
-__global__ void __launch_bounds__(kBlock) kSample(const __grid_constant__ DevGrid g,
-                                                  uint32_t maxDepth, uint64_t n,
-                                                  const float *__restrict__ pts, uint32_t attr,
-                                                  float *__restrict__ out)
+// ---------------------------------------------------------------------------
+// Spatially sorted tiles.  A CTA takes TILE consecutive query points, moves
+// them to index space, counting-sorts them in shared memory by a hash of
+// their 8^3 brick, computes them in that order and writes the results back
+// in the caller's order.  Consecutive points of a coherent batch (samples
+// along a ray) are several voxels apart, so without the sort every lane of a
+// warp gathers from a different cache line; after it, a warp's lanes share a
+// few bricks.  Results are unchanged: each point is computed by the same
+// code, only by a different thread.
+// ---------------------------------------------------------------------------
+constexpr int kTileThreads = 256;
+constexpr int kSortBins    = 1024;
+
+template <typename T>
+__device__ __forceinline__ DenseField<T> makeFieldAs(const DevGrid &g, uint32_t a, uint32_t,
+                                                     DenseField<T> *)
 {
-  const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n)
-    return;
-  const f3 p = xfmPoint(g.objectToIndex, loadPoint(pts, i));
-  float v;
-  if (DENSE)
-    v = filterAt<DenseField<T>, FILTER>(DenseField<T>(g, attr), g.constantCellData != 0, p);
-  else
-    v = filterAt<SparseField<T>, FILTER>(SparseField<T>(g, attr, maxDepth),
-                                         g.constantCellData != 0, p);
-  out[i] = v;
+  return DenseField<T>(g, a);
+}
+template <typename T>
+__device__ __forceinline__ SparseField<T> makeFieldAs(const DevGrid &g, uint32_t a, uint32_t depth,
+                                                      SparseField<T> *)
+{
+  return SparseField<T>(g, a, depth);
+}
+template <class Field>
+__device__ __forceinline__ Field makeField(const DevGrid &g, uint32_t attr, uint32_t maxDepth)
+{
+  return makeFieldAs(g, attr, maxDepth, (Field *)nullptr);
 }
 
-template <typename T, bool DENSE, int FILTER>
-__global__ void __launch_bounds__(kBlock) kGradient(const __grid_constant__ DevGrid g,
-                                                    uint32_t maxDepth, uint64_t n,
-                                                    const float *__restrict__ pts,
-                                                    uint32_t attr, float *__restrict__ out)
+// Sort key: hash of the point's 8^3 brick.  Only the grouping depends on
+// it, so the single-instruction round-down conversion is used.
+__device__ __forceinline__ uint32_t tileKey(f3 p)
 {
-  const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n)
-    return;
-  f3 r = {0.f, 0.f, 0.f};
-  if (FILTER != kFilterNearest) {
-    const f3 p = xfmPoint(g.objectToIndex, loadPoint(pts, i));
-    f3 gi;
-    if (DENSE) {
-      DenseField<T> F(g, attr);
-      gi = FILTER == kFilterCubic ? gradientCubic(F, p) : gradientLinear(F, p);
-    } else {
-      SparseField<T> F(g, attr, maxDepth);
-      gi = FILTER == kFilterCubic ? gradientCubic(F, p) : gradientLinear(F, p);
+  const uint32_t bx = (uint32_t)__float2int_rd(p.x) >> 3, by = (uint32_t)__float2int_rd(p.y) >> 3,
+                 bz = (uint32_t)__float2int_rd(p.z) >> 3;
+  return ((bx * 73856093u) ^ (by * 19349663u) ^ (bz * 83492791u)) & (kSortBins - 1);
+}
+
+template <typename T, bool DENSE, int FILTER, bool GRAD, int TILE>
+__global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constant__ DevGrid g,
+                                                            uint32_t maxDepth, uint64_t n,
+                                                            const float *__restrict__ pts,
+                                                            uint32_t attr, float *__restrict__ out)
+{
+  constexpr int PPT  = TILE / kTileThreads;
+  constexpr int OUTF = GRAD ? 3 : 1;
+  __shared__ float sx[TILE], sy[TILE], sz[TILE];
+  __shared__ uint16_t sidx[TILE];
+  __shared__ float res[TILE * OUTF];
+  __shared__ int hist[kSortBins];
+  const uint64_t base = (uint64_t)blockIdx.x * TILE;
+  const int cnt       = (int)min((uint64_t)TILE, n - base);
+  for (int k = threadIdx.x; k < kSortBins; k += kTileThreads)
+    hist[k] = 0;
+  f3 p[PPT];
+  uint32_t key[PPT];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < PPT; ++j) {
+    const int k = threadIdx.x + j * kTileThreads;
+    if (k < cnt) {
+      p[j]   = xfmPoint(g.objectToIndex, loadPoint(pts, base + k));
+      key[j] = tileKey(p[j]);
+      atomicAdd(&hist[key[j]], 1);
     }
-    r = xfmNormal(g.objectToIndex, gi);
   }
-  out[3 * i]     = r.x;
-  out[3 * i + 1] = r.y;
-  out[3 * i + 2] = r.z;
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan of the histogram by one warp
+    int run = 0;
+    for (int b = 0; b < kSortBins; b += 32) {
+      const int v = hist[b + threadIdx.x];
+      int incl    = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (threadIdx.x >= o)
+          incl += t;
+      }
+      hist[b + threadIdx.x] = run + incl - v;
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < PPT; ++j) {
+    const int k = threadIdx.x + j * kTileThreads;
+    if (k < cnt) {
+      const int pos = atomicAdd(&hist[key[j]], 1);
+      sx[pos]       = p[j].x;
+      sy[pos]       = p[j].y;
+      sz[pos]       = p[j].z;
+      sidx[pos]     = (uint16_t)k;
+    }
+  }
+  __syncthreads();
+  const bool cc = g.constantCellData != 0;
+  // field parameters read from the launch's constant bank once per thread
+  using Field = typename std::conditional<DENSE, DenseField<T>, SparseField<T>>::type;
+  const Field F = makeField<Field>(g, attr, maxDepth);
+  auto compute = [&](int j) {
+    const int k = threadIdx.x + j * kTileThreads;
+    if (k < cnt) {
+      const f3 q = {sx[k], sy[k], sz[k]};
+      const int o = sidx[k];
+      if (GRAD) {
+        f3 r = {0.f, 0.f, 0.f};
+        if (FILTER != kFilterNearest) {
+          const f3 gi = FILTER == kFilterCubic ? gradientCubic(F, q) : gradientLinear(F, q);
+          r = xfmNormal(g.objectToIndex, gi);
+        }
+        res[3 * o]     = r.x;
+        res[3 * o + 1] = r.y;
+        res[3 * o + 2] = r.z;
+      } else {
+        res[o] = filterAt<Field, FILTER>(F, cc, q);
+      }
+    }
+  };
+  // Unrolled, the loads of all PPT points of a thread are in flight at once;
+  // the 64-tap tricubic stays rolled to bound its register use.
+  if constexpr (FILTER == kFilterCubic) {
+#pragma unroll 1
+    for (int j = 0; j < PPT; ++j)
+      compute(j);
+  } else {
+#pragma unroll
+    for (int j = 0; j < PPT; ++j)
+      compute(j);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < cnt * OUTF; k += kTileThreads)
+    out[base * OUTF + k] = res[k];
 }
-
 
 template <typename T, bool DENSE, int FILTER>
 void launchTyped(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float *pts, uint32_t attr,
                  float *out, bool grad, cudaStream_t st)
 {
-  const dim3 grid((unsigned)((n + kBlock - 1) / kBlock));
-  if (grad)
-    kGradient<T, DENSE, FILTER><<<grid, kBlock, 0, st>>>(g, maxDepth, n, pts, attr, out);
-  else
-    kSample<T, DENSE, FILTER><<<grid, kBlock, 0, st>>>(g, maxDepth, n, pts, attr, out);
+  // 2048-point tiles for samples (40 KB shared), 1024 for gradients and the
+  // register-heavy tricubic.
+  if (grad) {
+    constexpr int TILE = 1024;
+    kSampleTile<T, DENSE, FILTER, true, TILE>
+        <<<(unsigned)((n + TILE - 1) / TILE), kTileThreads, 0, st>>>(g, maxDepth, n, pts, attr, out);
+  } else if (FILTER == kFilterCubic) {
+    constexpr int TILE = 1024;
+    kSampleTile<T, DENSE, FILTER, false, TILE>
+        <<<(unsigned)((n + TILE - 1) / TILE), kTileThreads, 0, st>>>(g, maxDepth, n, pts, attr, out);
+  } else {
+    constexpr int TILE = 2048;
+    kSampleTile<T, DENSE, FILTER, false, TILE>
+        <<<(unsigned)((n + TILE - 1) / TILE), kTileThreads, 0, st>>>(g, maxDepth, n, pts, attr, out);
+  }
 }
 
 // Type dispatch for one filter (defined per filter in k_sample_<filter>.cu).

@@ -37,7 +37,13 @@ __device__ __forceinline__ int32_t toIntX86(float x)
 {
   return (x >= -2147483648.f && x < 2147483648.f) ? (int32_t)x : INT32_MIN;
 }
-__device__ __forceinline__ int32_t ifloor(float x) { return toIntX86(floorf(x)); }
+// floor to int32 with the same out-of-range / NaN result (INT32_MIN); the
+// round-down conversion saturates, so only |x| >= 2^31 and NaN need fixing.
+__device__ __forceinline__ int32_t ifloor(float x)
+{
+  const int32_t i = __float2int_rd(x);
+  return fabsf(x) < 2147483648.f ? i : INT32_MIN;
+}
 
 __device__ __forceinline__ f3 xfmPoint(const float *M, f3 p)
 {
@@ -111,13 +117,16 @@ __device__ __forceinline__ float ldAny(uint32_t type, const void *p, uint64_t i)
 }
 
 // ---------------------------------------------------------------------------
-// Dense field: x-fastest array, out-of-domain taps read the background.
+// Dense field: bricked voxel array (brickIndex, grid.h); out-of-domain taps
+// read the background.  Which voxel a tap reads, and what it returns, is
+// exactly the reference's x-fastest dense load; only the address differs.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct DenseField {
   const T *data;
   uint32_t ax, ay, az;
   int32_t rx, ry, rz;
+  uint32_t sx, sy;
   float bg;
 
   __device__ __forceinline__ DenseField(const DevGrid &g, uint32_t a)
@@ -128,33 +137,48 @@ struct DenseField {
         rx(g.rootOrigin[0]),
         ry(g.rootOrigin[1]),
         rz(g.rootOrigin[2]),
+        sx(g.superX),
+        sy(g.superY),
         bg(g.background[a])
   {
+  }
+
+  // true if the 2^3 box at domain offset o lies in the domain and in one brick
+  __device__ __forceinline__ bool boxInBrick(uint32_t ox, uint32_t oy, uint32_t oz) const
+  {
+    return (ox < ax - 1) & (oy < ay - 1) & (oz < az - 1) & ((ox & 7u) != 7u) & ((oy & 7u) != 7u) &
+           ((oz & 7u) != 7u);
+  }
+
+  __device__ __forceinline__ uint64_t index(uint32_t ox, uint32_t oy, uint32_t oz) const
+  {
+    return brickIndex(ox, oy, oz, sx, sy);
   }
 
   __device__ __forceinline__ float at(int32_t x, int32_t y, int32_t z) const
   {
     const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
     if (ox < ax && oy < ay && oz < az)
-      return ldv(data, ((uint64_t)oz * ay + oy) * (uint64_t)ax + ox);
+      return ldv(data, index(ox, oy, oz));
     return bg;
   }
 
-  // The 8 trilinear corners s[4x+2y+z] at (x..x+1, y..y+1, z..z+1).
+  // The 8 trilinear corners s[4x+2y+z] at (x..x+1, y..y+1, z..z+1).  When
+  // the 2^3 box lies inside the domain and inside one brick, the corners sit
+  // at fixed offsets from the first one.
   __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
   {
     const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
-    if (ox + 1 < ax && oy + 1 < ay && oz + 1 < az && ox < ax && oy < ay && oz < az) {
-      const uint64_t sy = ax, sz = (uint64_t)ax * ay;
-      const T *b = data + (oz * sz + oy * sy + ox);
+    if (boxInBrick(ox, oy, oz)) {
+      const T *b = data + index(ox, oy, oz);
       s[0]       = ldv(b, 0);
       s[4]       = ldv(b, 1);
-      s[2]       = ldv(b, sy);
-      s[6]       = ldv(b, sy + 1);
-      s[1]       = ldv(b, sz);
-      s[5]       = ldv(b, sz + 1);
-      s[3]       = ldv(b, sz + sy);
-      s[7]       = ldv(b, sz + sy + 1);
+      s[2]       = ldv(b, 8);
+      s[6]       = ldv(b, 9);
+      s[1]       = ldv(b, 64);
+      s[5]       = ldv(b, 65);
+      s[3]       = ldv(b, 72);
+      s[7]       = ldv(b, 73);
     } else {
 #pragma unroll
       for (int o = 0; o < 8; ++o)
@@ -165,19 +189,9 @@ struct DenseField {
   // The 64 tricubic taps s[16x+4y+z] at offsets -1..2.
   __device__ __forceinline__ void stencil64(int32_t x, int32_t y, int32_t z, float s[64]) const
   {
-    const uint32_t ox = (uint32_t)(x - 1 - rx), oy = (uint32_t)(y - 1 - ry),
-                   oz = (uint32_t)(z - 1 - rz);
-    if (ox + 3 < ax && oy + 3 < ay && oz + 3 < az && ox < ax && oy < ay && oz < az) {
-      const uint64_t sy = ax, sz = (uint64_t)ax * ay;
-      const T *b = data + (oz * sz + oy * sy + ox);
 #pragma unroll
-      for (int o = 0; o < 64; ++o)
-        s[o] = ldv(b, (uint64_t)(o & 3) * sz + (uint64_t)((o >> 2) & 3) * sy + (o >> 4));
-    } else {
-#pragma unroll
-      for (int o = 0; o < 64; ++o)
-        s[o] = at(x + (o >> 4) - 1, y + ((o >> 2) & 3) - 1, z + (o & 3) - 1);
-    }
+    for (int o = 0; o < 64; ++o)
+      s[o] = at(x + (o >> 4) - 1, y + ((o >> 2) & 3) - 1, z + (o & 3) - 1);
   }
 };
 
