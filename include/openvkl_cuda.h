@@ -281,6 +281,28 @@ OPENVKL_CUDA_INTERFACE uint64_t vklCudaGetTreeLevel(VKLVolume volume, unsigned i
                                                     uint64_t *voxels, float *valueRanges,
                                                     uint32_t *origins);
 
+// EXTENSION (no counterpart in the reference): the value range that
+// vklGetValueRange would report for a structuredRegular volume of
+// dimensions (dimX, dimY, dimZ) over `voxels` (x-fastest, device memory,
+// type uchar / short / ushort / half / float / double) with the given
+// "background", written as {lower, upper} to `valueRange` (2 floats, device
+// memory) asynchronously on the device's stream.  It allocates no memory:
+// its scratch is a fixed static device array, which bounds the volume to
+// 16,777,216 leaves (8^3 voxel blocks, e.g. 2048^3 voxels); larger volumes
+// return VKL_INVALID_ARGUMENT before anything is launched.  The first call
+// on a device is a one-time set-up (it resolves the scratch and loads the
+// kernels) and belongs before any stream capture.  Calls whose work
+// overlaps on one device share the scratch and race: issue them on one
+// stream.  The calling thread's current CUDA device must be the VKL
+// device's.  For volumes with NaN voxels the result may differ from the
+// committed volume's, whose NaN handling depends on reduction order.
+// Returns VKL_NO_ERROR once launched, else the error code (also reported
+// through the device's error callback).
+OPENVKL_CUDA_INTERFACE VKLError vklCudaDenseValueRangeNoAlloc(VKLDevice device, const void *voxels,
+                                                             VKLDataType voxelType, int dimX,
+                                                             int dimY, int dimZ, float background,
+                                                             float *valueRange);
+
 #ifdef __cplusplus
 }
 #endif

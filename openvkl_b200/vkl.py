@@ -63,7 +63,7 @@ EXPORTS = [
     "vklInitHitIterator", "vklIterateHit", "vklIterateIntervalsN", "vklIterateHitsN",
     "vklNewVolumeObserver", "vklNewSamplerObserver", "vklMapObserver", "vklUnmapObserver",
     "vklGetObserverElementType", "vklGetObserverElementSize", "vklGetObserverNumElements",
-    "vklCudaGetTreeLevel",
+    "vklCudaGetTreeLevel", "vklCudaDenseValueRangeNoAlloc",
 ]
 
 
@@ -183,6 +183,7 @@ def load_library(path: str = LIB_PATH, load_only: bool = False) -> C.CDLL:
         "vklGetObserverElementSize": (SZ, [O]),
         "vklGetObserverNumElements": (SZ, [O]),
         "vklCudaGetTreeLevel": (C.c_uint64, [O, U, VP, VP, VP]),
+        "vklCudaDenseValueRangeNoAlloc": (I, [VP, VP, I, I, I, I, C.c_float, VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -437,6 +438,29 @@ def structured_regular(device: Device, data, grid_origin=None, grid_spacing=None
         v.set_data("data", Data(device, objects=datas))
     v.commit()
     return v
+
+
+def dense_value_range_no_alloc(device: Device, voxels, out, background=float("nan"),
+                               vkl_type: Optional[int] = None):
+    """vklCudaDenseValueRangeNoAlloc: the value range a structuredRegular
+    volume over `voxels` (a contiguous CUDA tensor shaped (Z, Y, X), x
+    fastest) would report, written as [lower, upper] into `out` (a CUDA
+    float32 tensor of 2 elements) on the device's stream, with no device
+    allocation.  Raises VKLError on a rejected call."""
+    import torch
+    tmap = {torch.float32: VKL_FLOAT, torch.float16: VKL_HALF, torch.uint8: VKL_UCHAR,
+            torch.int16: VKL_SHORT, torch.float64: VKL_DOUBLE}
+    assert voxels.is_contiguous() and voxels.dim() == 3
+    assert out.dtype == torch.float32 and out.is_contiguous() and out.numel() >= 2
+    t = vkl_type or tmap[voxels.dtype]
+    Z, Y, X = voxels.shape
+    device.pending = None
+    code = device.lib.vklCudaDenseValueRangeNoAlloc(device.handle, C.c_void_p(voxels.data_ptr()), t,
+                                                    X, Y, Z, float(background),
+                                                    C.c_void_p(out.data_ptr()))
+    if code != 0:
+        device.pending = None
+        raise VKLError(code, device.last_error()[1])
 
 
 def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, packed_tile=None,
