@@ -78,14 +78,32 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
 {
   constexpr int PPT  = TILE / kTileThreads;
   constexpr int OUTF = GRAD ? 3 : 1;
-  __shared__ float sx[TILE], sy[TILE], sz[TILE];
+  // sx | sy | sz; before the sort the same words hold the tile's points as
+  // the caller laid them out (x, y, z per point)
+  __shared__ __align__(16) float sxyz[3 * TILE];
+  float *const sx = sxyz, *const sy = sxyz + TILE, *const sz = sxyz + 2 * TILE;
   __shared__ uint16_t sidx[TILE];
   __shared__ float res[TILE * OUTF];
-  __shared__ int hist[kSortBins];
+  __shared__ __align__(16) int hist[kSortBins];
   const uint64_t base = (uint64_t)blockIdx.x * TILE;
   const int cnt       = (int)min((uint64_t)TILE, n - base);
   for (int k = threadIdx.x; k < kSortBins; k += kTileThreads)
     hist[k] = 0;
+  {
+    // the tile's 12-byte points are one contiguous run: load it with 16-byte
+    // loads when it is 16-byte aligned (whole tiles always are if pts is)
+    const float *src = pts + 3 * base;
+    const int nf     = 3 * cnt;
+    int k0           = 0;
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+      const int n4 = nf >> 2;
+      for (int k = threadIdx.x; k < n4; k += kTileThreads)
+        reinterpret_cast<float4 *>(sxyz)[k] = __ldcs(reinterpret_cast<const float4 *>(src) + k);
+      k0 = n4 << 2;
+    }
+    for (int k = k0 + threadIdx.x; k < nf; k += kTileThreads)
+      sxyz[k] = __ldcs(src + k);
+  }
   f3 p[PPT];
   uint32_t key[PPT];
   __syncthreads();
@@ -93,26 +111,35 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
   for (int j = 0; j < PPT; ++j) {
     const int k = threadIdx.x + j * kTileThreads;
     if (k < cnt) {
-      p[j]   = xfmPoint(g.objectToIndex, loadPoint(pts, base + k));
+      p[j]   = xfmPoint(g.objectToIndex, f3{sxyz[3 * k], sxyz[3 * k + 1], sxyz[3 * k + 2]});
       key[j] = tileKey(p[j]);
       atomicAdd(&hist[key[j]], 1);
     }
   }
   __syncthreads();
-  if (threadIdx.x < 32) {  // exclusive scan of the histogram by one warp
-    int run = 0;
-    for (int b = 0; b < kSortBins; b += 32) {
-      const int v = hist[b + threadIdx.x];
-      int incl    = v;
+  {
+    // exclusive scan of the histogram: 4 bins per thread, warp scans, then
+    // the warp totals
+    static_assert(kSortBins == 4 * kTileThreads, "scan layout");
+    __shared__ int warpSum[kTileThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int4 h   = reinterpret_cast<const int4 *>(hist)[threadIdx.x];
+    const int tot  = h.x + h.y + h.z + h.w;
+    int incl       = tot;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (threadIdx.x >= o)
-          incl += t;
-      }
-      hist[b + threadIdx.x] = run + incl - v;
-      run += __shfl_sync(0xffffffffu, incl, 31);
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o)
+        incl += t;
     }
+    if (lane == 31)
+      warpSum[warp] = incl;
+    __syncthreads();
+    int before = incl - tot;
+    for (int w = 0; w < warp; ++w)
+      before += warpSum[w];
+    reinterpret_cast<int4 *>(hist)[threadIdx.x] =
+        make_int4(before, before + h.x, before + h.x + h.y, before + h.x + h.y + h.z);
   }
   __syncthreads();
 #pragma unroll
@@ -163,7 +190,7 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
   }
   __syncthreads();
   for (int k = threadIdx.x; k < cnt * OUTF; k += kTileThreads)
-    out[base * OUTF + k] = res[k];
+    __stcs(out + base * OUTF + k, res[k]);
 }
 
 template <typename T, bool DENSE, int FILTER>

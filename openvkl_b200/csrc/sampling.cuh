@@ -126,7 +126,7 @@ struct DenseField {
   const T *data;
   uint32_t ax, ay, az;
   int32_t rx, ry, rz;
-  uint32_t sx, sy;
+  uint64_t yStride, zStride;  // supertile strides in elements: superX << 18, superX*superY << 18
   float bg;
 
   __device__ __forceinline__ DenseField(const DevGrid &g, uint32_t a)
@@ -137,61 +137,77 @@ struct DenseField {
         rx(g.rootOrigin[0]),
         ry(g.rootOrigin[1]),
         rz(g.rootOrigin[2]),
-        sx(g.superX),
-        sy(g.superY),
+        yStride((uint64_t)g.superX << 18),
+        zStride((uint64_t)g.superX * g.superY << 18),
         bg(g.background[a])
   {
   }
 
-  // true if the 2^3 box at domain offset o lies in the domain and in one brick
-  __device__ __forceinline__ bool boxInBrick(uint32_t ox, uint32_t oy, uint32_t oz) const
+  // brickIndex(x, y, z) is a sum of one term per axis (its bit fields do not
+  // overlap), so a stencil's addresses are sums of a few per-axis terms.
+  __device__ __forceinline__ uint64_t termX(uint32_t x) const
   {
-    return (ox < ax - 1) & (oy < ay - 1) & (oz < az - 1) & ((ox & 7u) != 7u) & ((oy & 7u) != 7u) &
-           ((oz & 7u) != 7u);
+    return ((uint64_t)(x >> 6) << 18) + (((x >> 3) & 7u) << 9) + (x & 7u);
   }
-
-  __device__ __forceinline__ uint64_t index(uint32_t ox, uint32_t oy, uint32_t oz) const
+  __device__ __forceinline__ uint64_t termY(uint32_t y) const
   {
-    return brickIndex(ox, oy, oz, sx, sy);
+    return (uint64_t)(y >> 6) * yStride + ((((y >> 3) & 7u) << 12) + ((y & 7u) << 3));
+  }
+  __device__ __forceinline__ uint64_t termZ(uint32_t z) const
+  {
+    return (uint64_t)(z >> 6) * zStride + ((((z >> 3) & 7u) << 15) + ((z & 7u) << 6));
   }
 
   __device__ __forceinline__ float at(int32_t x, int32_t y, int32_t z) const
   {
     const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
     if (ox < ax && oy < ay && oz < az)
-      return ldv(data, index(ox, oy, oz));
+      return ldv(data, termX(ox) + termY(oy) + termZ(oz));
     return bg;
   }
 
-  // The 8 trilinear corners s[4x+2y+z] at (x..x+1, y..y+1, z..z+1).  When
-  // the 2^3 box lies inside the domain and inside one brick, the corners sit
-  // at fixed offsets from the first one.
-  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  // The W^3 taps s[W*W*i + W*j + k] at (x+LO+i, y+LO+j, z+LO+k); taps outside
+  // the domain read the background.  Every lane issues the same W^3 loads
+  // (predicated), with no branch on where its stencil falls.
+  template <int W, int LO>
+  __device__ __forceinline__ void stencil(int32_t x, int32_t y, int32_t z, float *s) const
   {
     const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
-    if (boxInBrick(ox, oy, oz)) {
-      const T *b = data + index(ox, oy, oz);
-      s[0]       = ldv(b, 0);
-      s[4]       = ldv(b, 1);
-      s[2]       = ldv(b, 8);
-      s[6]       = ldv(b, 9);
-      s[1]       = ldv(b, 64);
-      s[5]       = ldv(b, 65);
-      s[3]       = ldv(b, 72);
-      s[7]       = ldv(b, 73);
-    } else {
+    uint64_t tx[W], ty[W], tz[W];
+    bool vx[W], vy[W], vz[W];
 #pragma unroll
-      for (int o = 0; o < 8; ++o)
-        s[o] = at(x + (o >> 2), y + ((o >> 1) & 1), z + (o & 1));
+    for (int i = 0; i < W; ++i) {
+      const uint32_t u = ox + (uint32_t)(LO + i), v = oy + (uint32_t)(LO + i),
+                     w = oz + (uint32_t)(LO + i);
+      vx[i] = u < ax;
+      vy[i] = v < ay;
+      vz[i] = w < az;
+      tx[i] = termX(u);
+      ty[i] = termY(v);
+      tz[i] = termZ(w);
     }
+#pragma unroll
+    for (int i = 0; i < W; ++i)
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const uint64_t xy = tx[i] + ty[j];
+        const bool ok     = vx[i] & vy[j];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          s[(i * W + j) * W + k] = (ok & vz[k]) ? ldv(data, xy + tz[k]) : bg;
+      }
+  }
+
+  // The 8 trilinear corners s[4x+2y+z] at (x..x+1, y..y+1, z..z+1).
+  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  {
+    stencil<2, 0>(x, y, z, s);
   }
 
   // The 64 tricubic taps s[16x+4y+z] at offsets -1..2.
   __device__ __forceinline__ void stencil64(int32_t x, int32_t y, int32_t z, float s[64]) const
   {
-#pragma unroll
-    for (int o = 0; o < 64; ++o)
-      s[o] = at(x + (o >> 4) - 1, y + ((o >> 2) & 3) - 1, z + (o & 3) - 1);
+    stencil<4, -1>(x, y, z, s);
   }
 };
 
