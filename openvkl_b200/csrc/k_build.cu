@@ -157,18 +157,18 @@ __global__ void __launch_bounds__(128) kSparseLeafRanges(const __grid_constant__
     if (!voxelIsLeaf(voxel)) {
       nlo = nhi = inDom ? 0.f : bgOut;
     } else if (voxelLeafFormat(voxel) == kFormatTile) {
-      nlo = nhi = ldv((const T *)g.tile[attr], voxelLeafIndex(voxel));
+      nlo = nhi = tileValue<T>(g, attr, voxelLeafIndex(voxel));
     } else {
       const uint32_t xa = ix == 0 ? 7 : 0, xb = ix == 2 ? 2 : 8;
       const uint32_t ya = iy == 0 ? 7 : 0, yb = iy == 2 ? 2 : 8;
       const uint32_t za = iz == 0 ? 7 : 0, zb = iz == 2 ? 2 : 8;
-      const T *base = (const T *)g.data[attr] + voxelLeafIndex(voxel) * 512;
+      const uint64_t li = voxelLeafIndex(voxel);
       nlo = kInf;
       nhi = -kInf;
       for (uint32_t x = xa; x < xb; ++x)
         for (uint32_t y = ya; y < yb; ++y)
           for (uint32_t z = za; z < zb; ++z) {
-            const float v = ldv(base, (x << 6) + (y << 3) + z);
+            const float v = packedLeafValue<T>(g, attr, li, li * 512 + (x << 6) + (y << 3) + z);
             nlo           = fminx(nlo, v);
             nhi           = fmaxx(nhi, v);
           }
@@ -293,6 +293,64 @@ __global__ void __launch_bounds__(1024) kVolumeRange(const __grid_constant__ Dev
   }
 }
 
+// ---------------------------------------------------------------------------
+// Leaf compression (extension): per packed leaf, offset = midpoint and
+// scale = half-range / code maximum of its non-NaN values, codes = the
+// round-to-nearest-even conversion of (v - offset) / scale.  One warp per
+// leaf, 16 values per lane.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void encodeCode(float r, __half *p) { *p = __float2half_rn(r); }
+__device__ __forceinline__ void encodeCode(float r, __nv_bfloat16 *p) { *p = __float2bfloat16_rn(r); }
+__device__ __forceinline__ void encodeCode(float r, __nv_fp8_storage_t *p)
+{
+  *p = __nv_cvt_float_to_fp8(r, __NV_SATFINITE, __NV_E4M3);
+}
+
+template <typename C>
+__global__ void __launch_bounds__(256) kCompressLeaves(const float *__restrict__ src, uint64_t numLeaves,
+                                                       float codeMax, C *__restrict__ codes,
+                                                       float2 *__restrict__ scaleOffset)
+{
+  const uint64_t leaf = (uint64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane      = threadIdx.x & 31;
+  if (leaf >= numLeaves)
+    return;
+  const float *v = src + leaf * 512;
+  float x[16];
+  float lo = kInf, hi = -kInf;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    x[i] = __ldg(v + lane + 32 * i);
+    if (x[i] < lo)
+      lo = x[i];
+    if (x[i] > hi)
+      hi = x[i];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+    if (l2 < lo)
+      lo = l2;
+    if (h2 > hi)
+      hi = h2;
+  }
+  lo += 0.f;  // one sign for zero
+  hi += 0.f;
+  float offset = 0.f, scale = 1.f;
+  if (lo <= hi) {
+    offset           = 0.5f * lo + 0.5f * hi;
+    const float half = 0.5f * hi - 0.5f * lo;
+    if (half > 0.f)
+      scale = half / codeMax;
+  }
+  if (lane == 0)
+    scaleOffset[leaf] = make_float2(scale, offset);
+  C *c = codes + leaf * 512;
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    encodeCode((x[i] - offset) / scale, c + lane + 32 * i);
+}
+
 inline unsigned blocksFor(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
 // x-fastest user array -> bricked copy; one thread per voxel, element size
@@ -359,7 +417,13 @@ void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
                             const uint32_t *leafOffsets, float *leafRanges, cudaStream_t st)
 {
   const unsigned grid = blocksFor(numLeaves, 128);
-  if (g.type[attr] == kHalf)
+  if (g.compress == kCompressFP16)
+    kSparseLeafRanges<CodeFP16><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.compress == kCompressBF16)
+    kSparseLeafRanges<CodeBF16><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.compress == kCompressFP8)
+    kSparseLeafRanges<CodeE4M3><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.type[attr] == kHalf)
     kSparseLeafRanges<__half><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
   else
     kSparseLeafRanges<float><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
@@ -395,6 +459,22 @@ uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &sup
   superY = (dims[1] + 63) / 64;
   const uint64_t superZ = (dims[2] + 63) / 64;
   return (uint64_t)superX * superY * superZ << 18;
+}
+
+void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,
+                          float *scaleOffset, cudaStream_t st)
+{
+  if (!numLeaves)
+    return;
+  const unsigned grid = blocksFor(numLeaves, 8);
+  float2 *so          = (float2 *)scaleOffset;
+  if (format == kCompressFP16)
+    kCompressLeaves<<<grid, 256, 0, st>>>(src, numLeaves, 1.f, (__half *)codes, so);
+  else if (format == kCompressBF16)
+    kCompressLeaves<<<grid, 256, 0, st>>>(src, numLeaves, 1.f, (__nv_bfloat16 *)codes, so);
+  else
+    kCompressLeaves<<<grid, 256, 0, st>>>(src, numLeaves, 448.f, (__nv_fp8_storage_t *)codes, so);
+  cudaCheck(cudaGetLastError(), "leaf compression kernel");
 }
 
 void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],

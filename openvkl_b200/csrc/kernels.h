@@ -20,6 +20,11 @@ void launchGradient(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
 
 // Bricked copy of a dense x-fastest voxel array (brickIndex, grid.h):
 // returns the element count of the bricked array and its supertile counts.
+// Compressed leaves: `numLeaves` packed float leaves (512 values each) ->
+// codes (2 or 1 bytes per value by `format`, kCompress*) and one
+// (scale, offset) float pair per leaf.
+void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,
+                          float *scaleOffset, cudaStream_t stream);
 uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY);
 void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
                      uint32_t superX, uint32_t superY, cudaStream_t stream);

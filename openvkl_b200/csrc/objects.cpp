@@ -640,6 +640,37 @@ void Volume::commitVdb()
       grid.type[a] = leafType;
     }
   }
+  // Compressed leaves (extension parameter "compression": "fp16" | "bf16" |
+  // "fp8"): float packed leaves are re-encoded on the GPU with one
+  // (scale, offset) pair per leaf; tiles stay float.
+  if (const Param *cp = find("compression")) {
+    const std::string &c = cp->str;
+    uint32_t fmt = kCompressNone;
+    if (c == "fp16")
+      fmt = kCompressFP16;
+    else if (c == "bf16")
+      fmt = kCompressBF16;
+    else if (c == "fp8" || c == "fp8_e4m3")
+      fmt = kCompressFP8;
+    else if (!(c.empty() || c == "none"))
+      fail("compression must be one of none, fp16, bf16, fp8");
+    if (fmt != kCompressNone) {
+      if (leafType != VKL_FLOAT)
+        fail("compression requires VKL_FLOAT leaves");
+      const uint64_t slots   = hasPacked ? nDense : numLeaves;
+      const size_t codeBytes = fmt == kCompressFP8 ? 1 : 2;
+      for (uint32_t a = 0; a < grid.numAttributes; ++a) {
+        DeviceBuffer *bc = newBuffer(std::max<uint64_t>(slots, 1) * 512 * codeBytes);
+        DeviceBuffer *bs = newBuffer(std::max<uint64_t>(slots, 1) * 8);
+        launchCompressLeaves(fmt, (const float *)grid.data[a], slots, bc->ptr, bs->as<float>(),
+                             device->stream);
+        grid.data[a]            = bc->ptr;
+        grid.leafScaleOffset[a] = bs->as<float>();
+      }
+      cudaCheck(cudaStreamSynchronize(device->stream), "leaf compression");
+    }
+    grid.compress = fmt;
+  }
   {
     std::vector<float> bg(grid.numAttributes, undefinedBackground());
     Data *bd = getData("background");

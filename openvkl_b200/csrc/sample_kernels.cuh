@@ -236,6 +236,16 @@ void dispatchFilter(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float
       return launchTyped<float, true, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
     }
   }
+  switch (g.compress) {
+  case kCompressFP16:
+    return launchTyped<CodeFP16, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  case kCompressBF16:
+    return launchTyped<CodeBF16, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  case kCompressFP8:
+    return launchTyped<CodeE4M3, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  default:
+    break;
+  }
   if (t == kHalf)
     return launchTyped<__half, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
   return launchTyped<float, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);

@@ -212,6 +212,75 @@ struct DenseField {
 };
 
 // ---------------------------------------------------------------------------
+// Leaf codecs of sparse volumes.  T = float / __half: the leaf arrays hold the
+// values.  The Code* tags: compressed leaves (an extension, no reference
+// counterpart) hold FP16 / BF16 / FP8-E4M3 codes, value = code * scale +
+// offset with one (scale, offset) pair per packed leaf, decoded in FP32;
+// tiles stay float.
+// ---------------------------------------------------------------------------
+struct CodeFP16 {};
+struct CodeBF16 {};
+struct CodeE4M3 {};
+
+template <typename T>
+struct LeafCodec {
+  static constexpr bool kScaled = false;
+  using Tile                    = T;
+  using Code                    = T;
+};
+template <>
+struct LeafCodec<CodeFP16> {
+  static constexpr bool kScaled = true;
+  using Tile                    = float;
+  using Code                    = __half;
+};
+template <>
+struct LeafCodec<CodeBF16> {
+  static constexpr bool kScaled = true;
+  using Tile                    = float;
+  using Code                    = __nv_bfloat16;
+};
+template <>
+struct LeafCodec<CodeE4M3> {
+  static constexpr bool kScaled = true;
+  using Tile                    = float;
+  using Code                    = __nv_fp8_storage_t;
+};
+
+__device__ __forceinline__ float ldCode(const __half *p, uint64_t i)
+{
+  return __half2float(__ldg(p + i));
+}
+__device__ __forceinline__ float ldCode(const __nv_bfloat16 *p, uint64_t i)
+{
+  return __bfloat162float(__ldg(p + i));
+}
+__device__ __forceinline__ float ldCode(const __nv_fp8_storage_t *p, uint64_t i)
+{
+  return __half2float(__half(__nv_cvt_fp8_to_halfraw(__ldg(p + i), __NV_E4M3)));
+}
+
+// Value of voxel vi of packed leaf li (vi counts from the start of the leaf array).
+template <typename T>
+__device__ __forceinline__ float packedLeafValue(const DevGrid &g, uint32_t attr, uint64_t li,
+                                                 uint64_t vi)
+{
+  if constexpr (LeafCodec<T>::kScaled) {
+    const float code = ldCode((const typename LeafCodec<T>::Code *)g.data[attr], vi);
+    const float2 so  = __ldg((const float2 *)g.leafScaleOffset[attr] + li);
+    return code * so.x + so.y;
+  } else {
+    return ldv((const T *)g.data[attr], vi);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ float tileValue(const DevGrid &g, uint32_t attr, uint64_t li)
+{
+  return ldv((const typename LeafCodec<T>::Tile *)g.tile[attr], li);
+}
+
+// ---------------------------------------------------------------------------
 // Sparse field: 4-level tree walk, packed leaves, tiles, error voxels.
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -253,9 +322,9 @@ struct SparseField {
     if (voxelIsLeaf(voxel)) {
       const uint64_t li = voxelLeafIndex(voxel);
       if (voxelLeafFormat(voxel) == kFormatTile)
-        return ldv((const T *)g.tile[attr], li);
+        return tileValue<T>(g, attr, li);
       const uint64_t vi = li * 512 + ((uint64_t)(ox & 7u) << 6) + ((oy & 7u) << 3) + (oz & 7u);
-      return ldv((const T *)g.data[attr], vi);
+      return packedLeafValue<T>(g, attr, li, vi);
     } else if (voxelIsError(voxel)) {
       const uint32_t level = (uint32_t)((voxel >> 8) & 0xffu);
       const uint32_t off   = (uint32_t)(voxel >> 32);
@@ -472,6 +541,16 @@ __device__ __forceinline__ float sampleIndexAny(const DevGrid &g, int filter, ui
     default:
       return sampleFiltered(DenseField<float>(g, attr), filter, cc, p);
     }
+  }
+  switch (g.compress) {
+  case kCompressFP16:
+    return sampleFiltered(SparseField<CodeFP16>(g, attr, depth), filter, cc, p);
+  case kCompressBF16:
+    return sampleFiltered(SparseField<CodeBF16>(g, attr, depth), filter, cc, p);
+  case kCompressFP8:
+    return sampleFiltered(SparseField<CodeE4M3>(g, attr, depth), filter, cc, p);
+  default:
+    break;
   }
   if (t == kHalf)
     return sampleFiltered(SparseField<__half>(g, attr, depth), filter, cc, p);

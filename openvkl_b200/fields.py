@@ -254,3 +254,79 @@ def shell_leaves(domain=256, shells=3, thickness=0.02, seed=5, leaf_frac_target=
     noise = _value_noise(vox, seed)
     values = np.clip(dens * (0.5 + noise), 0.0, 1.0).astype(np.float32)
     return origins, values.reshape(-1)
+
+
+def _value_noise_torch(p, seed, octaves=4):
+    """Torch twin of `_value_noise` (float32 positions, same hash)."""
+    import torch
+    total = torch.zeros(p.shape[:-1], dtype=torch.float32, device=p.device)
+    norm = 0.0
+    for o in range(octaves):
+        freq = 2.0 ** o / 64.0
+        amp = 0.5 ** o
+        q = p * freq
+        i = torch.floor(q).to(torch.int64)
+        f = q - i
+        f = f * f * (3 - 2 * f)
+        acc = torch.zeros_like(total)
+        for c in range(8):
+            dx, dy, dz = c >> 2, (c >> 1) & 1, c & 1
+            h = ((i[..., 0] + dx) * 73856093) ^ ((i[..., 1] + dy) * 19349663) ^ \
+                ((i[..., 2] + dz) * 83492791) ^ (seed * 2654435761 + o)
+            h = (h * 0x27d4eb2d) & 0xffffffff
+            val = (h >> 8).to(torch.float32) / float(1 << 24)
+            w = (f[..., 0] if dx else 1 - f[..., 0]) * (f[..., 1] if dy else 1 - f[..., 1]) * \
+                (f[..., 2] if dz else 1 - f[..., 2])
+            acc += w * val
+        total += amp * acc
+        norm += amp
+    return total / norm
+
+
+def shell_vdb_torch(domain=4096, leaf_fraction=0.05, thickness=0.02, seed=5, device="cuda",
+                    max_shells=64):
+    """Sparse VDB leaves of seeded spherical shells (radius U[0.1, 0.45] x
+    domain, relative thickness `thickness`) with fractal-noise density in
+    [0, 1], built in GPU memory.  Shells are added in seed order until at
+    least `leaf_fraction` of the (domain/8)^3 leaf slots are active.
+
+    Returns (origins (L,3) int32 numpy, values (L*512,) float32 CUDA tensor,
+    z fastest inside each leaf, shells used, active fraction)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    n = domain // 8
+    half = 0.5 * thickness * domain
+    lim = half + 4 * math.sqrt(3)
+    centers, radii = [], []
+    active = torch.zeros((n, n, n), dtype=torch.bool, device=device)
+    g = torch.arange(n, device=device, dtype=torch.float32) * 8 + 4.0
+    frac = 0.0
+    while frac < leaf_fraction and len(centers) < max_shells:
+        c = rng.uniform(0.3, 0.7, size=3) * domain
+        r = rng.uniform(0.1, 0.45) * domain
+        centers.append(c)
+        radii.append(r)
+        for xi in range(0, n, 64):  # slabs keep the temporaries small
+            dx = (g[xi:xi + 64, None, None] - c[0]) ** 2
+            dist = torch.sqrt(dx + (g[None, :, None] - c[1]) ** 2 + (g[None, None, :] - c[2]) ** 2)
+            active[xi:xi + 64] |= (dist - r).abs() <= lim
+        frac = float(active.sum().item()) / n ** 3
+    idx = torch.nonzero(active)                      # (L, 3) in (x, y, z) slot order
+    origins = (idx * 8).to(torch.int32)
+    L = origins.shape[0]
+    values = torch.empty((L, 512), dtype=torch.float32, device=device)
+    off = torch.stack(torch.meshgrid(torch.arange(8, device=device), torch.arange(8, device=device),
+                                     torch.arange(8, device=device), indexing="ij"), -1).reshape(-1, 3)
+    C = torch.tensor(np.array(centers), dtype=torch.float32, device=device)
+    R = torch.tensor(np.array(radii), dtype=torch.float32, device=device)
+    chunk = 1 << 15
+    for s in range(0, L, chunk):
+        e = min(L, s + chunk)
+        vox = origins[s:e, None, :].to(torch.float32) + off[None].to(torch.float32) + 0.5
+        dens = torch.zeros(vox.shape[:2], dtype=torch.float32, device=device)
+        for k in range(C.shape[0]):
+            dist = torch.linalg.norm(vox - C[k], dim=2)
+            dens = torch.maximum(dens, torch.clamp(1.0 - (dist - R[k]).abs() / half, 0.0, 1.0))
+        noise = _value_noise_torch(vox, seed)
+        values[s:e] = torch.clamp(dens * (0.5 + noise), 0.0, 1.0)
+    return origins.cpu().numpy(), values.reshape(-1), len(centers), frac

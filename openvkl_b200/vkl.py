@@ -305,6 +305,10 @@ class _Obj:
         self.lib.vklSetVec3i(self.h, name.encode(), *[int(x) for x in v])
         return self
 
+    def set_string(self, name, v):
+        self.lib.vklSetString(self.h, name.encode(), str(v).encode())
+        return self
+
     def set_data(self, name, data: "Data"):
         self.lib.vklSetData(self.h, name.encode(), data.h)
         self._keep.append(data)
@@ -464,9 +468,12 @@ def dense_value_range_no_alloc(device: Device, voxels, out, background=float("na
 
 
 def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, packed_tile=None,
-               node_data=None, index_to_object=None, index_clipping_bounds=None, background=None):
+               node_data=None, index_to_object=None, index_clipping_bounds=None, background=None,
+               compression=None):
     """A committed vdb volume from packed leaves (nodesPackedDense / Tile, one
-    array or a list per attribute) or per-leaf node.data arrays."""
+    array or a list per attribute) or per-leaf node.data arrays.
+    `compression` ("fp16" | "bf16" | "fp8") stores float leaves as codes with
+    a per-leaf scale and offset (cuda device extension)."""
     v = Volume(device, "vdb")
     v.set_data("node.level", Data(device, np.ascontiguousarray(levels, np.uint32)))
     v.set_data("node.origin", Data(device, np.ascontiguousarray(origins, np.int32).reshape(-1),
@@ -486,6 +493,8 @@ def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, pack
         v.set_param("indexClippingBounds", VKL_BOX3I, np.asarray(index_clipping_bounds, np.int32))
     if background is not None:
         v.set_data("background", Data(device, np.asarray(background, np.float32).reshape(-1)))
+    if compression is not None:
+        v.set_string("compression", compression)
     v.commit()
     return v
 

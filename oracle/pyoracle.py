@@ -86,6 +86,8 @@ def lib(fast: bool = False) -> C.CDLL:
         L.orc_tricubic_map.argtypes = [P, P, P]
         L.orc_inner_nodes.restype = U64
         L.orc_inner_nodes.argtypes = [P, U32, U32, U64, P]
+        L.orc_round_format.argtypes = [C.c_int, U64, P, P]
+        L.orc_quantize_leaves.argtypes = [C.c_int, U64, P, P, P]
         _libs[name] = L
     return _libs[name]
 
@@ -256,3 +258,25 @@ def tricubic_map():
     w = np.zeros(nnz, np.float32)
     L.orc_tricubic_map(_p(start), _p(cols), _p(w))
     return start, cols, w
+
+
+COMPRESSION_FORMATS = {"fp16": 1, "bf16": 2, "fp8": 3}
+
+
+def round_format(fmt, values):
+    """Each float rounded to nearest-even in fp16 / bf16 / fp8 (E4M3, saturating)."""
+    x = np.ascontiguousarray(values, np.float32)
+    out = np.empty_like(x)
+    lib().orc_round_format(COMPRESSION_FORMATS[fmt], x.size, _p(x), _p(out))
+    return out
+
+
+def quantize_leaves(fmt, leaves):
+    """Packed leaves (n*512 floats) -> (decoded floats, (n,2) scale/offset) as
+    the cuda device's compressed storage reproduces them."""
+    x = np.ascontiguousarray(leaves, np.float32).reshape(-1)
+    n = x.size // 512
+    dec = np.empty_like(x)
+    so = np.empty((n, 2), np.float32)
+    lib().orc_quantize_leaves(COMPRESSION_FORMATS[fmt], n, _p(x), _p(dec), _p(so))
+    return dec, so

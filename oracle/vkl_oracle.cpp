@@ -1806,3 +1806,82 @@ uint64_t orc_inner_nodes(const OrcVolume *v, uint32_t maxDepth, uint32_t attr, u
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Compressed leaves (extension of the cuda device, test restatement).
+// Round to nearest, ties to even, to a binary format with `mant` stored
+// mantissa bits and minimum normal exponent `emin` (subnormals below it):
+// the value is a multiple of the format's spacing at its exponent, so
+// scaling by that power of two and rounding to an integer is exact in double.
+// ---------------------------------------------------------------------------
+namespace {
+
+float roundToFormat(float x, int mant, int emin, float maxFinite, bool saturate)
+{
+  if (std::isnan(x) || x == 0.f)
+    return x;
+  const float a = std::fabs(x);
+  if (std::isinf(a))
+    return saturate ? std::copysign(maxFinite, x) : x;
+  int e = 0;
+  std::frexp(a, &e);  // a = f * 2^e, f in [0.5, 1)
+  int E = e - 1;
+  if (E < emin)
+    E = emin;
+  const double q = std::ldexp(1.0, E - mant);
+  double r       = std::nearbyint((double)a / q) * q;
+  if (r > (double)maxFinite)
+    r = saturate ? (double)maxFinite : (double)INFINITY;
+  return std::copysign((float)r, x);
+}
+
+float roundFormat(int format, float x)
+{
+  switch (format) {
+  case 1:
+    return roundToFormat(x, 10, -14, 65504.f, false);
+  case 2:
+    return roundToFormat(x, 7, -126, 3.38953139e38f, false);
+  default:
+    return roundToFormat(x, 3, -6, 448.f, true);
+  }
+}
+
+}  // namespace
+
+void orc_round_format(int format, uint64_t n, const float *in, float *out)
+{
+  for (uint64_t i = 0; i < n; ++i)
+    out[i] = roundFormat(format, in[i]);
+}
+
+void orc_quantize_leaves(int format, uint64_t numLeaves, const float *in, float *decoded,
+                         float *scaleOffset)
+{
+  const float codeMax = format == 3 ? 448.f : 1.f;
+  for (uint64_t l = 0; l < numLeaves; ++l) {
+    const float *v = in + l * 512;
+    float lo = std::numeric_limits<float>::infinity(), hi = -lo;
+    for (int i = 0; i < 512; ++i) {
+      if (v[i] < lo)
+        lo = v[i];
+      if (v[i] > hi)
+        hi = v[i];
+    }
+    lo += 0.f;
+    hi += 0.f;
+    float offset = 0.f, scale = 1.f;
+    if (lo <= hi) {
+      offset           = 0.5f * lo + 0.5f * hi;
+      const float half = 0.5f * hi - 0.5f * lo;
+      if (half > 0.f)
+        scale = half / codeMax;
+    }
+    scaleOffset[2 * l]     = scale;
+    scaleOffset[2 * l + 1] = offset;
+    for (int i = 0; i < 512; ++i) {
+      const float code       = roundFormat(format, (v[i] - offset) / scale);
+      decoded[l * 512 + i]   = code * scale + offset;
+    }
+  }
+}

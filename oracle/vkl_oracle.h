@@ -160,6 +160,20 @@ uint64_t orc_inner_nodes(const OrcVolume *v,
                          uint64_t cap,
                          float *out);
 
+// Compressed leaves (the cuda device's extension; no reference
+// counterpart).  format: 1 = FP16, 2 = BF16, 3 = FP8-E4M3 (saturating).
+// orc_round_format: each input rounded to nearest-even in the format,
+// returned as float.  orc_quantize_leaves: per leaf of 512 values,
+// offset = 0.5*lo + 0.5*hi and scale = (0.5*hi - 0.5*lo) / codeMax over the
+// non-NaN values (scale 1 for a constant leaf); decoded = round((v - offset)
+// / scale) * scale + offset in float; scaleOffset gets 2 floats per leaf.
+void orc_round_format(int format, uint64_t n, const float *in, float *out);
+void orc_quantize_leaves(int format,
+                         uint64_t numLeaves,
+                         const float *in,
+                         float *decoded,
+                         float *scaleOffset);
+
 #ifdef __cplusplus
 }
 #endif
