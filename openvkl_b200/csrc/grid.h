@@ -134,6 +134,12 @@ struct DevGrid {
   // attribute; value = code * scale + offset.
   uint32_t compress;
   const float *leafScaleOffset[kMaxAttributes];
+  // Sparse: flat leaf map over the active domain at leaf resolution, x
+  // fastest: entry = the voxel code the full-depth tree walk reaches for
+  // that 8^3 leaf slot (leaf, tile or empty).  Null when it would exceed its
+  // memory budget; the walk is used then, and for maxSamplingDepth < 3.
+  const uint64_t *leafMap;
+  uint32_t leafMapDims[3];
 };
 
 struct DevSampler {

@@ -294,6 +294,24 @@ __global__ void __launch_bounds__(1024) kVolumeRange(const __grid_constant__ Dev
 }
 
 // ---------------------------------------------------------------------------
+// Flat leaf map: for every 8^3 leaf slot of the active domain, the voxel code
+// the full-depth walk reaches (VdbSampler_traverseAndSample.ih:85-306 at
+// maxSamplingDepth 3).  Built once at commit so sampling replaces the
+// three dependent node loads of the walk by one load.
+// ---------------------------------------------------------------------------
+__global__ void kBuildLeafMap(const __grid_constant__ DevGrid g, uint3 dims, uint64_t *__restrict__ map)
+{
+  const uint64_t i     = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t total = (uint64_t)dims.x * dims.y * dims.z;
+  if (i >= total)
+    return;
+  const uint32_t lx = (uint32_t)(i % dims.x), ly = (uint32_t)((i / dims.x) % dims.y),
+                 lz = (uint32_t)(i / ((uint64_t)dims.x * dims.y));
+  const SparseField<float> F(g, 0, kNumLevels - 1);
+  map[i] = F.walk(lx * 8, ly * 8, lz * 8);
+}
+
+// ---------------------------------------------------------------------------
 // Leaf compression (extension): per packed leaf, offset = midpoint and
 // scale = half-range / code maximum of its non-NaN values, codes = the
 // round-to-nearest-even conversion of (v - offset) / scale.  One warp per
@@ -459,6 +477,15 @@ uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &sup
   superY = (dims[1] + 63) / 64;
   const uint64_t superZ = (dims[2] + 63) / 64;
   return (uint64_t)superX * superY * superZ << 18;
+}
+
+void launchBuildLeafMap(const DevGrid &g, uint64_t *map, cudaStream_t st)
+{
+  const uint3 d = {g.leafMapDims[0], g.leafMapDims[1], g.leafMapDims[2]};
+  const uint64_t n = (uint64_t)d.x * d.y * d.z;
+  if (n)
+    kBuildLeafMap<<<blocksFor(n, 256), 256, 0, st>>>(g, d, map);
+  cudaCheck(cudaGetLastError(), "leaf map kernel");
 }
 
 void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,

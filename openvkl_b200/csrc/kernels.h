@@ -18,13 +18,16 @@ void launchSample(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
 void launchGradient(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
                     const float *points, uint32_t attr, float *out, cudaStream_t stream);
 
-// Bricked copy of a dense x-fastest voxel array (brickIndex, grid.h):
-// returns the element count of the bricked array and its supertile counts.
+// Flat leaf map of a sparse grid (g.leafMapDims set, g.leafMap unused):
+// map[slot] = full-depth walk result per 8^3 leaf slot, x fastest.
+void launchBuildLeafMap(const DevGrid &g, uint64_t *map, cudaStream_t stream);
 // Compressed leaves: `numLeaves` packed float leaves (512 values each) ->
 // codes (2 or 1 bytes per value by `format`, kCompress*) and one
 // (scale, offset) float pair per leaf.
 void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,
                           float *scaleOffset, cudaStream_t stream);
+// Bricked copy of a dense x-fastest voxel array (brickIndex, grid.h):
+// returns the element count of the bricked array and its supertile counts.
 uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY);
 void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
                      uint32_t superX, uint32_t superY, cudaStream_t stream);

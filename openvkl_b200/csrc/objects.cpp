@@ -219,6 +219,9 @@ const uint8_t *Data::hostBytes()
 // ---------------------------------------------------------------------------
 namespace {
 
+// Device memory a sparse volume may spend on its flat leaf map.
+constexpr uint64_t kLeafMapBudgetBytes = 4ull << 30;
+
 bool isVoxelType(VKLDataType t)
 {
   return t == VKL_UCHAR || t == VKL_SHORT || t == VKL_USHORT || t == VKL_HALF ||
@@ -805,6 +808,23 @@ void Volume::commitVdb()
     grid.levels[l] = {numNodes[l], bo->as<uint32_t>(), bv->as<uint64_t>(), br->as<float>()};
   }
   levelNodes[3] = numLeaves;
+
+  // Flat leaf map (sampling replaces the walk by one load) when it fits its
+  // budget; parameter "leafMap" (bool, default true) turns it off.
+  {
+    uint64_t slots = 1;
+    for (int a = 0; a < 3; ++a) {
+      grid.leafMapDims[a] = (grid.activeSize[a] + 7) / 8;
+      slots *= grid.leafMapDims[a];
+    }
+    if (getBool("leafMap", true) && slots * 8 <= kLeafMapBudgetBytes) {
+      DeviceBuffer *bm = newBuffer(std::max<uint64_t>(slots, 1) * 8);
+      launchBuildLeafMap(grid, bm->as<uint64_t>(), device->stream);
+      grid.leafMap = bm->as<uint64_t>();
+    } else {
+      grid.leafMapDims[0] = grid.leafMapDims[1] = grid.leafMapDims[2] = 0;
+    }
+  }
 
   DeviceBuffer dOff, dLeafVoxel, leafRanges, volRange;
   dOff.alloc(off.size() * 4);

@@ -294,9 +294,19 @@ struct SparseField {
   {
   }
 
+  // The voxel holding the leaf that contains the (in-domain, root-relative)
+  // offset: one load from the flat leaf map at full depth, else the walk.
+  __device__ __forceinline__ uint64_t traverse(uint32_t ox, uint32_t oy, uint32_t oz) const
+  {
+    if (g.leafMap && maxDepth >= kNumLevels - 1)
+      return __ldg(g.leafMap + ((uint64_t)(oz >> 3) * g.leafMapDims[1] + (oy >> 3)) * g.leafMapDims[0] +
+                   (ox >> 3));
+    return walk(ox, oy, oz);
+  }
+
   // Walk from the root to the voxel holding the leaf that contains the
   // (in-domain, root-relative) offset.
-  __device__ __forceinline__ uint64_t traverse(uint32_t ox, uint32_t oy, uint32_t oz) const
+  __device__ __forceinline__ uint64_t walk(uint32_t ox, uint32_t oy, uint32_t oz) const
   {
     const uint32_t lx = ox & ~7u, ly = oy & ~7u, lz = oz & ~7u;
     uint64_t node = 0;
@@ -316,15 +326,35 @@ struct SparseField {
     return 0;
   }
 
+  // (scale, offset) of the packed leaf a voxel code points at; (1, 0) for
+  // uncompressed leaves and everything else.
+  __device__ __forceinline__ float2 leafScale(uint64_t voxel) const
+  {
+    if constexpr (LeafCodec<T>::kScaled) {
+      if (voxelIsLeaf(voxel) && voxelLeafFormat(voxel) != kFormatTile)
+        return __ldg((const float2 *)g.leafScaleOffset[attr] + voxelLeafIndex(voxel));
+    }
+    return make_float2(1.f, 0.f);
+  }
+
   __device__ __forceinline__ float leafValue(uint64_t voxel, uint32_t ox, uint32_t oy,
                                              uint32_t oz) const
+  {
+    return leafValueWith(voxel, leafScale(voxel), ox, oy, oz);
+  }
+
+  __device__ __forceinline__ float leafValueWith(uint64_t voxel, float2 so, uint32_t ox,
+                                                 uint32_t oy, uint32_t oz) const
   {
     if (voxelIsLeaf(voxel)) {
       const uint64_t li = voxelLeafIndex(voxel);
       if (voxelLeafFormat(voxel) == kFormatTile)
         return tileValue<T>(g, attr, li);
       const uint64_t vi = li * 512 + ((uint64_t)(ox & 7u) << 6) + ((oy & 7u) << 3) + (oz & 7u);
-      return packedLeafValue<T>(g, attr, li, vi);
+      if constexpr (LeafCodec<T>::kScaled)
+        return ldCode((const typename LeafCodec<T>::Code *)g.data[attr], vi) * so.x + so.y;
+      else
+        return ldv((const T *)g.data[attr], vi);
     } else if (voxelIsError(voxel)) {
       const uint32_t level = (uint32_t)((voxel >> 8) & 0xffu);
       const uint32_t off   = (uint32_t)(voxel >> 32);
@@ -359,7 +389,46 @@ struct SparseField {
     const uint32_t bx = (uint32_t)(x + LO - g.rootOrigin[0]),
                    by = (uint32_t)(y + LO - g.rootOrigin[1]),
                    bz = (uint32_t)(z + LO - g.rootOrigin[2]);
+    if constexpr (W == 2) {
+      // 2^3 corners: along an axis the second corner is in the next leaf
+      // only when the first sits on the leaf's last voxel.  Leaf slot s
+      // (bit 2 = x, 1 = y, 0 = z) is needed when its bits are a subset of
+      // the crossing axes; each corner selects its slot with static selects,
+      // so the codes stay in registers.
+      const bool cx = (bx & 7u) == 7u, cy = (by & 7u) == 7u, cz = (bz & 7u) == 7u;
+      const bool inx[2] = {bx < g.activeSize[0], bx + 1 < g.activeSize[0]};
+      const bool iny[2] = {by < g.activeSize[1], by + 1 < g.activeSize[1]};
+      const bool inz[2] = {bz < g.activeSize[2], bz + 1 < g.activeSize[2]};
+      uint64_t code[8];
+      float2 sc[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
+        const bool need = (!i || cx) && (!j || cy) && (!k || cz) && inx[i] && iny[j] && inz[k];
+        code[q] = need ? traverse(bx + i, by + j, bz + k) : 0ull;
+        sc[q]   = need ? leafScale(code[q]) : make_float2(1.f, 0.f);
+      }
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {
+        const int i = o >> 2, j = (o >> 1) & 1, k = o & 1;
+        const uint32_t ox = bx + i, oy = by + j, oz = bz + k;
+        if (!(inx[i] && iny[j] && inz[k])) {
+          s[o] = g.background[attr];
+          continue;
+        }
+        const bool ux = i && cx, uy = j && cy, uz = k && cz;
+        const uint64_t c0 = uz ? code[1] : code[0], c1 = uz ? code[3] : code[2],
+                       c2 = uz ? code[5] : code[4], c3 = uz ? code[7] : code[6];
+        const float2 f0 = uz ? sc[1] : sc[0], f1 = uz ? sc[3] : sc[2], f2 = uz ? sc[5] : sc[4],
+                     f3 = uz ? sc[7] : sc[6];
+        const uint64_t cv = ux ? (uy ? c3 : c2) : (uy ? c1 : c0);
+        const float2 fv   = ux ? (uy ? f3 : f2) : (uy ? f1 : f0);
+        s[o]              = leafValueWith(cv, fv, ox, oy, oz);
+      }
+      return;
+    }
     uint64_t cache[8];
+    float2 scale[8];
     uint32_t have = 0;
 #pragma unroll
     for (int o = 0; o < W * W * W; ++o) {
@@ -373,9 +442,10 @@ struct SparseField {
                             (((oy & ~7u) != (by & ~7u)) << 1) | ((oz & ~7u) != (bz & ~7u));
       if (!(have & (1u << slot))) {
         cache[slot] = traverse(ox, oy, oz);
+        scale[slot] = leafScale(cache[slot]);
         have |= 1u << slot;
       }
-      s[o] = leafValue(cache[slot], ox, oy, oz);
+      s[o] = leafValueWith(cache[slot], scale[slot], ox, oy, oz);
     }
   }
 

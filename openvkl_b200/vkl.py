@@ -469,7 +469,7 @@ def dense_value_range_no_alloc(device: Device, voxels, out, background=float("na
 
 def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, packed_tile=None,
                node_data=None, index_to_object=None, index_clipping_bounds=None, background=None,
-               compression=None):
+               compression=None, leaf_map=None):
     """A committed vdb volume from packed leaves (nodesPackedDense / Tile, one
     array or a list per attribute) or per-leaf node.data arrays.
     `compression` ("fp16" | "bf16" | "fp8") stores float leaves as codes with
@@ -495,6 +495,8 @@ def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, pack
         v.set_data("background", Data(device, np.asarray(background, np.float32).reshape(-1)))
     if compression is not None:
         v.set_string("compression", compression)
+    if leaf_map is not None:
+        v.set_bool("leafMap", leaf_map)
     v.commit()
     return v
 

@@ -60,6 +60,23 @@ def test_sparse_tree_and_sampling_bit_exact(vkl, device, oracle, dtype):
         np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts, filter=fv)))
 
 
+def test_tree_walk_equals_leaf_map(vkl, device, oracle):
+    # sampling normally reads the flat leaf map; with it turned off every tap
+    # walks the tree: both must give the oracle's results
+    origins, levels, formats, vals, tvals = _shell_vdb(domain=96, seed=12)
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    pts = (origins[np.random.default_rng(2).integers(0, len(origins), 20000)]
+           + np.random.default_rng(3).uniform(-3, 11, (20000, 3))).astype(np.float32)
+    for leaf_map in (True, False):
+        vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tvals,
+                             leaf_map=leaf_map)
+        _check_tree(vol, ref)
+        for fv in (0, 100, 200):
+            smp = vkl.Sampler(vol, filter=fv, gradient_filter=fv)
+            np.testing.assert_array_equal(bits(smp.sample(pts)), bits(ref.sample(pts, filter=fv)))
+            np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts, filter=fv)))
+
+
 @pytest.mark.parametrize("depth", [0, 1, 2])
 def test_max_sampling_depth(vkl, device, oracle, depth):
     origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=9)
