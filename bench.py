@@ -483,11 +483,13 @@ def main(argv=None):
     ap.add_argument("--no-extras", action="store_true",
                     help="timed loop only (no e2e / roofline bytes / CPU baseline): profiling runs")
     ap.add_argument("--small", action="store_true",
-                    help="512^3 volume, 480x270 rays x 256: the ncu capture case")
+                    help="512^3 volume, 480x270 rays x 256 (vdb: 2048^3 domain, 2^24 points): "
+                         "the ncu capture case")
     args = ap.parse_args(argv)
     if args.small:
-        global DIMS, WIDTH, HEIGHT, INCOHERENT_N
+        global DIMS, WIDTH, HEIGHT, INCOHERENT_N, VDB_DOMAIN, VDB_POINTS
         DIMS, WIDTH, HEIGHT, INCOHERENT_N = (512, 512, 512), 480, 270, 1 << 24
+        VDB_DOMAIN, VDB_POINTS = 2048, 1 << 24
     if args.no_extras:
         args.no_cpu_baseline = True
     if args.impl == "reference":
