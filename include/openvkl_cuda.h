@@ -281,6 +281,42 @@ OPENVKL_CUDA_INTERFACE uint64_t vklCudaGetTreeLevel(VKLVolume volume, unsigned i
                                                     uint64_t *voxels, float *valueRanges,
                                                     uint32_t *origins);
 
+// EXTENSION (no counterpart in the reference): batched multi-volume
+// sampling.  One job = a committed sampler, `numPoints` object-space points
+// and outputs for samples (`numPoints` floats) and / or gradients
+// (`numPoints` vec3f), all in device memory (an output may be NULL).  The
+// batch records every job into one CUDA graph: dense volumes and plain
+// sparse volumes with the trilinear filter run in persistent kernels that
+// compute each point's sample and gradient from one gather; other jobs run
+// as the vklComputeSampleN / vklComputeGradientN launches.  Results equal
+// those calls bit for bit.  `autotune` != 0 times candidate tile sizes,
+// brick sorting and CTAs per SM on the batch and keeps the fastest
+// (remembered for later batches of the same shape).  Running enqueues the
+// graph on the device's stream; the job list is fixed at creation (the
+// points and outputs are re-read at every run).
+typedef struct {
+  VKLSampler sampler;
+  const vkl_vec3f *points;
+  unsigned int numPoints;
+  unsigned int attributeIndex;
+  float *samples;
+  vkl_vec3f *gradients;
+} VKLCudaSampleJob;
+
+typedef struct VKLCudaSampleBatch_ *VKLCudaSampleBatch;
+
+OPENVKL_CUDA_INTERFACE VKLCudaSampleBatch vklCudaNewSampleBatch(VKLDevice device,
+                                                                unsigned int numJobs,
+                                                                const VKLCudaSampleJob *jobs,
+                                                                int autotune);
+OPENVKL_CUDA_INTERFACE VKLError vklCudaRunSampleBatch(VKLCudaSampleBatch batch);
+// The configuration the batch runs its largest fused class with, and how
+// many jobs are fused (the rest run as plain launches).
+OPENVKL_CUDA_INTERFACE VKLError vklCudaGetSampleBatchConfig(VKLCudaSampleBatch batch,
+                                                           int *tilePoints, int *sorted,
+                                                           int *ctasPerSM, int *fusedJobs);
+OPENVKL_CUDA_INTERFACE void vklCudaReleaseSampleBatch(VKLCudaSampleBatch batch);
+
 // EXTENSION (no counterpart in the reference): the value range that
 // vklGetValueRange would report for a structuredRegular volume of
 // dimensions (dimX, dimY, dimZ) over `voxels` (x-fastest, device memory,

@@ -47,23 +47,26 @@ def sinusoid_field(dims, seed=1, noise=0.05, dtype=np.float32):
 
 
 def sinusoid_field_torch(dims, seed=1, noise=0.05, device="cuda"):
-    """Same distribution as sinusoid_field, generated slab by slab on the GPU."""
+    """Same distribution as sinusoid_field, generated on the GPU in slabs of
+    about 2^24 voxels."""
     import torch
     X, Y, Z = dims
     freq, amp, phase = _sinusoid_params(seed)
     g = torch.Generator(device=device)
     g.manual_seed(seed + 1000)
     out = torch.empty((Z, Y, X), dtype=torch.float32, device=device)
-    x = torch.arange(X, device=device, dtype=torch.float32)[None, :] / X
-    y = torch.arange(Y, device=device, dtype=torch.float32)[:, None] / Y
-    for zi in range(Z):
-        zz = zi / Z
-        acc = torch.zeros((Y, X), device=device, dtype=torch.float32)
+    x = torch.arange(X, device=device, dtype=torch.float32)[None, None, :] / X
+    y = torch.arange(Y, device=device, dtype=torch.float32)[None, :, None] / Y
+    step = max(1, (1 << 24) // (X * Y))
+    for z0 in range(0, Z, step):
+        z1 = min(Z, z0 + step)
+        zz = torch.arange(z0, z1, device=device, dtype=torch.float32)[:, None, None] / Z
+        acc = torch.zeros((z1 - z0, Y, X), device=device, dtype=torch.float32)
         for k in range(4):
             acc += float(amp[k]) * torch.sin(2 * math.pi * (float(freq[k, 0]) * x + float(freq[k, 1]) * y
                                                            + float(freq[k, 2]) * zz) + float(phase[k]))
-        acc += (torch.rand((Y, X), generator=g, device=device) * 2 - 1) * noise
-        out[zi] = acc
+        acc += (torch.rand((z1 - z0, Y, X), generator=g, device=device) * 2 - 1) * noise
+        out[z0:z1] = acc
     return out
 
 

@@ -64,6 +64,8 @@ EXPORTS = [
     "vklNewVolumeObserver", "vklNewSamplerObserver", "vklMapObserver", "vklUnmapObserver",
     "vklGetObserverElementType", "vklGetObserverElementSize", "vklGetObserverNumElements",
     "vklCudaGetTreeLevel", "vklCudaDenseValueRangeNoAlloc",
+    "vklCudaNewSampleBatch", "vklCudaRunSampleBatch", "vklCudaGetSampleBatchConfig",
+    "vklCudaReleaseSampleBatch",
 ]
 
 
@@ -96,6 +98,11 @@ class VKLInterval(C.Structure):
 
 class VKLHit(C.Structure):
     _fields_ = [("t", C.c_float), ("sample", C.c_float), ("epsilon", C.c_float)]
+
+
+class VKLCudaSampleJob(C.Structure):
+    _fields_ = [("sampler", VKLObject), ("points", C.c_void_p), ("numPoints", C.c_uint),
+                ("attributeIndex", C.c_uint), ("samples", C.c_void_p), ("gradients", C.c_void_p)]
 
 
 class vvec3f4(C.Structure):
@@ -184,6 +191,10 @@ def load_library(path: str = LIB_PATH, load_only: bool = False) -> C.CDLL:
         "vklGetObserverNumElements": (SZ, [O]),
         "vklCudaGetTreeLevel": (C.c_uint64, [O, U, VP, VP, VP]),
         "vklCudaDenseValueRangeNoAlloc": (I, [VP, VP, I, I, I, I, C.c_float, VP]),
+        "vklCudaNewSampleBatch": (VP, [VP, U, C.POINTER(VKLCudaSampleJob), I]),
+        "vklCudaRunSampleBatch": (I, [VP]),
+        "vklCudaGetSampleBatchConfig": (I, [VP, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+        "vklCudaReleaseSampleBatch": (None, [VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -465,6 +476,56 @@ def dense_value_range_no_alloc(device: Device, voxels, out, background=float("na
     if code != 0:
         device.pending = None
         raise VKLError(code, device.last_error()[1])
+
+
+class SampleBatch:
+    """vklCudaNewSampleBatch: a fixed list of (sampler, points, outputs) jobs
+    run as one CUDA graph.  jobs: iterable of (sampler, points, samples,
+    gradients[, attr]) with CUDA tensors (samples / gradients may be None)."""
+
+    def __init__(self, device: Device, jobs, autotune=False):
+        self.device = device
+        self.lib = device.lib
+        arr = (VKLCudaSampleJob * len(jobs))()
+        self._keep = []
+        for i, job in enumerate(jobs):
+            smp, pts, smps, grads = job[:4]
+            attr = job[4] if len(job) > 4 else 0
+            arr[i].sampler = smp.h
+            arr[i].points = pts.data_ptr()
+            arr[i].numPoints = pts.shape[0]
+            arr[i].attributeIndex = attr
+            arr[i].samples = None if smps is None else smps.data_ptr()
+            arr[i].gradients = None if grads is None else grads.data_ptr()
+            self._keep.append((smp, pts, smps, grads))
+        device.pending = None
+        self.h = self.lib.vklCudaNewSampleBatch(device.handle, len(jobs), arr, int(bool(autotune)))
+        if not self.h:
+            device.raise_pending()
+            raise VKLError(*device.last_error())
+
+    def run(self):
+        code = self.lib.vklCudaRunSampleBatch(self.h)
+        if code != 0:
+            self.device.pending = None
+            raise VKLError(code, self.device.last_error()[1])
+
+    def config(self):
+        t, s, c, f = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.lib.vklCudaGetSampleBatchConfig(self.h, C.byref(t), C.byref(s), C.byref(c), C.byref(f))
+        return {"tile_points": t.value, "sorted": bool(s.value), "ctas_per_sm": c.value,
+                "fused_jobs": f.value}
+
+    def release(self):
+        if self.h:
+            self.lib.vklCudaReleaseSampleBatch(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, packed_tile=None,
