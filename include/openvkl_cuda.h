@@ -317,6 +317,58 @@ OPENVKL_CUDA_INTERFACE VKLError vklCudaGetSampleBatchConfig(VKLCudaSampleBatch b
                                                            int *ctasPerSM, int *fusedJobs);
 OPENVKL_CUDA_INTERFACE void vklCudaReleaseSampleBatch(VKLCudaSampleBatch batch);
 
+// EXTENSION (no counterpart in the reference): learned surrogate of a
+// volume.  A 16-level hash-grid encoding (2^log2TableSize entries of 2 FP16
+// features per level, resolution floor(baseResolution * growth^level) over
+// the volume's object bounding box) feeds a 32-64-64-64-1 ReLU MLP (FP16
+// weights, tensor cores).  The sampler must be trilinear over float voxels;
+// its plain samples are the training targets, the fallback and the judge of
+// the surrogate's error.  Parameters (host or device memory): the table as
+// levels x entries x 2 floats, the weights as W1 (64x32), W2 (64x64),
+// W3 (64x64), W4 (64), row-major, concatenated (10304 floats).  Points,
+// targets, samples and the train-step loss are device memory.
+typedef struct VKLCudaSurrogate_ *VKLCudaSurrogate;
+
+OPENVKL_CUDA_INTERFACE VKLCudaSurrogate vklCudaNewSurrogate(VKLSampler sampler,
+                                                            unsigned int log2TableSize,
+                                                            float baseResolution, float growth);
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateSetParameters(VKLCudaSurrogate surrogate,
+                                                             const float *table,
+                                                             const float *weights);
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGetParameters(VKLCudaSurrogate surrogate,
+                                                             float *table, float *weights);
+// Gradients of sum((y - target)^2) over the n points (no update); outputs in
+// host or device memory, any may be NULL.
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGradient(VKLCudaSurrogate surrogate,
+                                                        unsigned int n,
+                                                        const vkl_vec3f *points,
+                                                        const float *targets, float *loss,
+                                                        float *tableGradient,
+                                                        float *weightGradient);
+// One Adam step (beta 0.9 / 0.99) on the loss sum((y - target)^2) / n;
+// `loss` (device, may be NULL) receives the sum of squared errors.
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateTrainStep(VKLCudaSurrogate surrogate,
+                                                         unsigned int n, const vkl_vec3f *points,
+                                                         const float *targets, float learningRate,
+                                                         float *loss);
+// Flags every 32^3-voxel region where |surrogate - plain sampler| exceeds
+// `threshold` at one of the points, or that none of the points reached.
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateCalibrate(VKLCudaSurrogate surrogate,
+                                                         unsigned int n, const vkl_vec3f *points,
+                                                         float threshold,
+                                                         unsigned int *flaggedRegions);
+// Surrogate samples; with `fallback` != 0 the plain sample in flagged regions
+// and outside the volume's domain (every region is flagged until calibrated).
+OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateSample(VKLCudaSurrogate surrogate, unsigned int n,
+                                                      const vkl_vec3f *points, float *samples,
+                                                      int fallback);
+OPENVKL_CUDA_INTERFACE void vklCudaGetSurrogateInfo(VKLCudaSurrogate surrogate,
+                                                    uint64_t *tableEntries,
+                                                    unsigned int *numWeights,
+                                                    uint64_t *numRegions,
+                                                    unsigned int *levelResolutions);
+OPENVKL_CUDA_INTERFACE void vklCudaReleaseSurrogate(VKLCudaSurrogate surrogate);
+
 // EXTENSION (no counterpart in the reference): the value range that
 // vklGetValueRange would report for a structuredRegular volume of
 // dimensions (dimX, dimY, dimZ) over `voxels` (x-fastest, device memory,

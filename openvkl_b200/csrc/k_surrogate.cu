@@ -1,0 +1,931 @@
+// Learned surrogate of a volume (extension; no reference counterpart).
+//
+// A multi-resolution hash-grid encoding (16 levels, 2 FP16 features per
+// entry, per-level resolution floor(base * growth^l), direct indexing while
+// (res+1)^3 fits the table, else the spatial hash) feeds a 32-64-64-64-1 ReLU
+// MLP without biases, FP16 weights and activations on the tensor cores
+// (mma.sync m16n8k16, FP32 accumulation).  It is trained on samples of the
+// plain sampler (the caller supplies points and the plain samples as
+// targets), with the loss sum (y - target)^2 / n and Adam.  The plain sampler
+// is also the judge: calibration evaluates both on caller-supplied points
+// and flags every 32^3-voxel region whose largest error exceeds a threshold
+// (or that no calibration point reached); sampling with fallback returns the
+// plain sample there and outside the volume's domain.
+//
+// Inference fuses the encoding and the MLP: a CTA encodes 128 points into
+// shared memory, each warp runs 32 of them through the MLP with the
+// activations kept in registers (an m16n8 accumulator tile is, after ReLU and
+// FP16 packing, exactly the A fragment of the next layer's m16n8k16 step).
+// Training runs forward and backward per 128-point tile in one kernel:
+// weight gradients as tensor-core products of the stored activations and
+// backward signals over the tile's points, encoding gradients scattered into
+// the table's gradient with float2 atomics; a separate kernel applies Adam to
+// the FP32 master parameters and refreshes their FP16 copies.
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "kernels.h"
+#include "objects.h"
+#include "sampling.cuh"
+
+namespace vklcuda {
+
+namespace {
+
+constexpr int kLv = 16;
+constexpr int kIn = 2 * kLv;  // 32 encoded features
+constexpr int kH  = 64;
+constexpr int kOffW1 = 0, kOffW2 = kH * kIn, kOffW3 = kOffW2 + kH * kH, kOffW4 = kOffW3 + kH * kH;
+constexpr int kNumW  = kOffW4 + kH;  // 10304
+constexpr int kTile  = 128;          // points per CTA tile
+constexpr int kThr   = 128;          // 4 warps x 32 points
+constexpr int kRegionLog = 5;        // 32^3-voxel calibration regions
+
+struct Encoding {
+  float lo[3], inv[3];
+  uint32_t res[kLv];
+  uint32_t dense[kLv];
+  uint32_t tableMask;
+  uint32_t tableSize;
+};
+
+struct Judge {
+  // plain-sampler fallback and calibration regions (index space)
+  uint32_t regionDims[3];
+  const uint8_t *flags;
+  float *regionErr;
+  uint32_t *regionSeen;
+  uint32_t attr;
+};
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1)
+{
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t ld32(const __half *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+__device__ __forceinline__ uint32_t pack(float lo, float hi)
+{
+  const __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// A fragment of the 16x16 block at (m0, k0) of row-major A (leading dim ld).
+__device__ __forceinline__ void loadA(uint32_t a[4], const __half *A, int ld, int m0, int k0, int g, int t)
+{
+  a[0] = ld32(A + (m0 + g) * ld + k0 + 2 * t);
+  a[1] = ld32(A + (m0 + g + 8) * ld + k0 + 2 * t);
+  a[2] = ld32(A + (m0 + g) * ld + k0 + 8 + 2 * t);
+  a[3] = ld32(A + (m0 + g + 8) * ld + k0 + 8 + 2 * t);
+}
+
+// B fragment of the 16x8 block (k0, n0) given B transposed, Bt[n][k] row-major.
+__device__ __forceinline__ void loadB(uint32_t &b0, uint32_t &b1, const __half *Bt, int ld, int n0, int k0,
+                                      int g, int t)
+{
+  b0 = ld32(Bt + (n0 + g) * ld + k0 + 2 * t);
+  b1 = ld32(Bt + (n0 + g) * ld + k0 + 8 + 2 * t);
+}
+
+// ReLU'd accumulators of 8 n-tiles (64 columns) -> A fragments of 4 k-steps.
+__device__ __forceinline__ void chain(const float acc[8][4], uint32_t a[4][4])
+{
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a[kk][0] = pack(fmaxf(acc[2 * kk][0], 0.f), fmaxf(acc[2 * kk][1], 0.f));
+    a[kk][1] = pack(fmaxf(acc[2 * kk][2], 0.f), fmaxf(acc[2 * kk][3], 0.f));
+    a[kk][2] = pack(fmaxf(acc[2 * kk + 1][0], 0.f), fmaxf(acc[2 * kk + 1][1], 0.f));
+    a[kk][3] = pack(fmaxf(acc[2 * kk + 1][2], 0.f), fmaxf(acc[2 * kk + 1][3], 0.f));
+  }
+}
+
+// Per-level cell of a point in [0,1]^3: integer corner and fraction.
+__device__ __forceinline__ void levelCell(const Encoding &E, int l, const float u[3], uint32_t i[3], float f[3])
+{
+  const float r = (float)E.res[l];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float x = u[a] * r;
+    const float fl = fminf(floorf(x), r - 1.f);
+    i[a]           = (uint32_t)fl;
+    f[a]           = x - fl;
+  }
+}
+
+__device__ __forceinline__ uint32_t entryOf(const Encoding &E, int l, uint32_t cx, uint32_t cy, uint32_t cz)
+{
+  if (E.dense[l]) {
+    const uint32_t r1 = E.res[l] + 1;
+    return cx + cy * r1 + cz * r1 * r1;
+  }
+  return (cx ^ (cy * 2654435761u) ^ (cz * 805459861u)) & E.tableMask;
+}
+
+__device__ __forceinline__ float cornerWeight(int c, const float f[3])
+{
+  const float wx = (c & 4) ? f[0] : 1.f - f[0];
+  const float wy = (c & 2) ? f[1] : 1.f - f[1];
+  const float wz = (c & 1) ? f[2] : 1.f - f[2];
+  return (wx * wy) * wz;
+}
+
+__device__ __forceinline__ void unitPosition(const Encoding &E, f3 p, float u[3])
+{
+  const float q[3] = {p.x, p.y, p.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    u[a] = fminf(fmaxf((q[a] - E.lo[a]) * E.inv[a], 0.f), 1.f);
+}
+
+// Encodes one point into 32 FP16 features (out: 16 half2 slots).
+__device__ __forceinline__ void encodePoint(const Encoding &E, const __half2 *__restrict__ table, const float u[3],
+                                            __half2 *out)
+{
+#pragma unroll 2
+  for (int l = 0; l < kLv; ++l) {
+    uint32_t i[3];
+    float f[3];
+    levelCell(E, l, u, i, f);
+    const __half2 *tl = table + (size_t)l * E.tableSize;
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t e = entryOf(E, l, i[0] + ((c >> 2) & 1), i[1] + ((c >> 1) & 1), i[2] + (c & 1));
+      const float w    = cornerWeight(c, f);
+      const float2 v   = __half22float2(__ldg(tl + e));
+      s0 += w * v.x;
+      s1 += w * v.y;
+    }
+    out[l] = __floats2half2_rn(s0, s1);
+  }
+}
+
+// Index-space region of an object-space point, or -1 outside the domain.
+__device__ __forceinline__ int64_t regionOf(const DevGrid &g, const Judge &J, f3 p)
+{
+  const f3 q = xfmPoint(g.objectToIndex, p);
+  const uint32_t ox = (uint32_t)(ifloor(q.x) - g.rootOrigin[0]), oy = (uint32_t)(ifloor(q.y) - g.rootOrigin[1]),
+                 oz = (uint32_t)(ifloor(q.z) - g.rootOrigin[2]);
+  if (!(ox < g.activeSize[0] && oy < g.activeSize[1] && oz < g.activeSize[2]))
+    return -1;
+  return ((int64_t)(oz >> kRegionLog) * J.regionDims[1] + (oy >> kRegionLog)) * J.regionDims[0] +
+         (ox >> kRegionLog);
+}
+
+template <class Field>
+__device__ __forceinline__ float plainSample(const DevGrid &g, const Judge &J, f3 p)
+{
+  const Field F = [&]() {
+    if constexpr (std::is_same<Field, DenseField<float>>::value)
+      return DenseField<float>(g, J.attr);
+    else
+      return SparseField<float>(g, J.attr, kNumLevels - 1);
+  }();
+  return sampleLinear(F, xfmPoint(g.objectToIndex, p));
+}
+
+// Shared weights of the forward pass (row-major [out][in], padded rows).
+struct FwdWeights {
+  __half w1[kH][kIn + 8];
+  __half w2[kH][kH + 8];
+  __half w3[kH][kH + 8];
+  __half w4[8][kH + 8];  // row 0 = W4, rows 1..7 zero (n8 tile)
+};
+
+__device__ __forceinline__ void loadFwdWeights(FwdWeights &W, const __half *__restrict__ w16)
+{
+  for (int k = threadIdx.x; k < kH * kIn; k += blockDim.x)
+    W.w1[k / kIn][k % kIn] = w16[kOffW1 + k];
+  for (int k = threadIdx.x; k < kH * kH; k += blockDim.x) {
+    W.w2[k / kH][k % kH] = w16[kOffW2 + k];
+    W.w3[k / kH][k % kH] = w16[kOffW3 + k];
+  }
+  for (int k = threadIdx.x; k < 8 * kH; k += blockDim.x)
+    W.w4[k / kH][k % kH] = k < kH ? w16[kOffW4 + k] : __float2half(0.f);
+}
+
+// Forward of one 16-row chunk (rows m0..m0+15 of X); returns the outputs of
+// rows m0+g and m0+g+8 in lanes with t == 0.  When HT is given, the FP16
+// activations of each hidden layer are also stored transposed: HT[l][col][row].
+__device__ __forceinline__ void forwardChunk(const FwdWeights &W, const __half *X, int ldx, int m0, int g, int t,
+                                             float &y0, float &y1, __half *HT, int ldh)
+{
+  uint32_t a[4][4];
+  float acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+  for (int kk = 0; kk < 2; ++kk) {
+    uint32_t ax[4];
+    loadA(ax, X, ldx, m0, 16 * kk, g, t);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      uint32_t b0, b1;
+      loadB(b0, b1, &W.w1[0][0], kIn + 8, 8 * j, 16 * kk, g, t);
+      mma16816(acc[j], ax, b0, b1);
+    }
+  }
+#pragma unroll
+  for (int layer = 0; layer < 3; ++layer) {
+    chain(acc, a);
+    if (HT) {
+      __half *H = HT + (size_t)layer * kH * ldh;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = 8 * j + 2 * t;
+        const __half2 lo = *reinterpret_cast<const __half2 *>(&a[j >> 1][(j & 1) ? 2 : 0]);
+        const __half2 hi = *reinterpret_cast<const __half2 *>(&a[j >> 1][(j & 1) ? 3 : 1]);
+        H[c * ldh + m0 + g]           = __low2half(lo);
+        H[(c + 1) * ldh + m0 + g]     = __high2half(lo);
+        H[c * ldh + m0 + g + 8]       = __low2half(hi);
+        H[(c + 1) * ldh + m0 + g + 8] = __high2half(hi);
+      }
+    }
+    if (layer == 2)
+      break;
+    const __half *Wl = layer == 0 ? &W.w2[0][0] : &W.w3[0][0];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        uint32_t b0, b1;
+        loadB(b0, b1, Wl, kH + 8, 8 * j, 16 * kk, g, t);
+        mma16816(acc[j], a[kk], b0, b1);
+      }
+  }
+  float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    uint32_t b0, b1;
+    loadB(b0, b1, &W.w4[0][0], kH + 8, 0, 16 * kk, g, t);
+    mma16816(o, a[kk], b0, b1);
+  }
+  y0 = o[0];
+  y1 = o[2];
+}
+
+// ---------------------------------------------------------------------------
+// Inference (optionally with the plain fallback) and calibration.
+// MODE 0: samples; MODE 1: calibration (region error of the network).
+// ---------------------------------------------------------------------------
+template <class Field, int MODE>
+__global__ void __launch_bounds__(kThr) kSurrogateInfer(const __grid_constant__ Encoding E,
+                                                        const __half2 *__restrict__ table,
+                                                        const __half *__restrict__ w16,
+                                                        const __grid_constant__ DevGrid g,
+                                                        const __grid_constant__ Judge J, uint64_t n,
+                                                        const float *__restrict__ pts, float *__restrict__ out,
+                                                        int fallback)
+{
+  __shared__ FwdWeights W;
+  __shared__ __align__(16) __half X[kTile][kIn + 8];
+  __shared__ float ys[kTile];
+  loadFwdWeights(W, w16);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+  for (uint64_t base = (uint64_t)blockIdx.x * kTile; base < n; base += (uint64_t)gridDim.x * kTile) {
+    const uint64_t i = base + threadIdx.x;
+    f3 p             = {0.f, 0.f, 0.f};
+    __half2 *row     = reinterpret_cast<__half2 *>(&X[threadIdx.x][0]);
+    if (i < n) {
+      p = {__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2)};
+      float u[3];
+      unitPosition(E, p, u);
+      encodePoint(E, table, u, row);
+    } else {
+      for (int k = 0; k < kLv; ++k)
+        row[k] = __floats2half2_rn(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int m0 = 32 * warp + 16 * c;
+      float y0, y1;
+      forwardChunk(W, &X[0][0], kIn + 8, m0, gq, tq, y0, y1, nullptr, 0);
+      if (tq == 0) {
+        ys[m0 + gq]     = y0;
+        ys[m0 + gq + 8] = y1;
+      }
+    }
+    __syncthreads();
+    if (i < n) {
+      float y = ys[threadIdx.x];
+      if (MODE == 0) {
+        if (fallback) {
+          const int64_t r = regionOf(g, J, p);
+          if (r < 0 || J.flags[r])
+            y = plainSample<Field>(g, J, p);
+        }
+        out[i] = y;
+      } else {
+        const int64_t r = regionOf(g, J, p);
+        const float ref = plainSample<Field>(g, J, p);
+        if (r >= 0 && !isnan(ref)) {
+          const float err = fabsf(y - ref);
+          atomicMax(reinterpret_cast<unsigned int *>(J.regionErr) + r, __float_as_uint(isnan(err) ? INFINITY : err));
+          J.regionSeen[r] = 1u;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void kRegionFlags(uint64_t n, const float *regionErr, const uint32_t *seen, float threshold,
+                             uint8_t *flags, unsigned int *flagged)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  const bool f = !seen[i] || !(regionErr[i] <= threshold);
+  flags[i]     = f ? 1 : 0;
+  if (f)
+    atomicAdd(flagged, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Training: forward + backward of 128-point tiles.
+// ---------------------------------------------------------------------------
+constexpr int kLdT = kTile + 8;  // transposed buffers: [col][row]
+constexpr int kLdR = kH + 8;     // row-major [row][64]
+
+struct TrainSmem {
+  FwdWeights W;
+  __half w1t[kIn][kH + 8];   // W1 transposed [in][out]
+  __half w2t[kH][kH + 8];
+  __half w3t[kH][kH + 8];
+  float w4[kH];
+  __half X[kTile][kIn + 8];
+  __half XT[kIn][kLdT];
+  __half HT[3][kH][kLdT];    // hidden activations, transposed
+  __half G[kTile][kLdR];     // backward signal, row-major
+  __half GT[kH][kLdT];       // and transposed
+  float u[kTile][3];
+  float dy[kTile];
+  float loss[kThr / 32];
+};
+
+// dW (64 x N) += GT (64 x 128) * BT (N x 128)^T for output rows 16w..16w+15.
+template <int NT>
+__device__ __forceinline__ void weightGrad(const TrainSmem &S, const __half *BT, int warp, int g, int t,
+                                           float *__restrict__ gW, int ldw)
+{
+  float acc[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; ++j)
+    acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+  for (int kk = 0; kk < kTile / 16; ++kk) {
+    uint32_t a[4];
+    loadA(a, &S.GT[0][0], kLdT, 16 * warp, 16 * kk, g, t);
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      uint32_t b0, b1;
+      loadB(b0, b1, BT, kLdT, 8 * j, 16 * kk, g, t);
+      mma16816(acc[j], a, b0, b1);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NT; ++j) {
+    const int r = 16 * warp + g, c = 8 * j + 2 * t;
+    atomicAdd(gW + r * ldw + c, acc[j][0]);
+    atomicAdd(gW + r * ldw + c + 1, acc[j][1]);
+    atomicAdd(gW + (r + 8) * ldw + c, acc[j][2]);
+    atomicAdd(gW + (r + 8) * ldw + c + 1, acc[j][3]);
+  }
+}
+
+// Backward signal of the previous layer for this warp's 32 rows:
+// acc[c][j] = (G * Wt^T) restricted to rows 32w+16c.., NT n-tiles.
+template <int NT>
+__device__ __forceinline__ void signalGrad(const TrainSmem &S, const __half *Wt, int warp, int g, int t,
+                                           float acc[2][NT][4])
+{
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+      acc[c][j][0] = acc[c][j][1] = acc[c][j][2] = acc[c][j][3] = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < kH / 16; ++kk) {
+      uint32_t a[4];
+      loadA(a, &S.G[0][0], kLdR, 32 * warp + 16 * c, 16 * kk, g, t);
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        uint32_t b0, b1;
+        loadB(b0, b1, Wt, kH + 8, 8 * j, 16 * kk, g, t);
+        mma16816(acc[c][j], a, b0, b1);
+      }
+    }
+  }
+}
+
+// G <- ReLU-masked signal (mask from the stored activations HT[col][row]).
+__device__ __forceinline__ void storeSignal(TrainSmem &S, const float acc[2][8][4], const __half *H, int warp,
+                                            int g, int t)
+{
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = 32 * warp + 16 * c + g, col = 8 * j + 2 * t;
+      const float v0 = __half2float(H[col * kLdT + r]) > 0.f ? acc[c][j][0] : 0.f;
+      const float v1 = __half2float(H[(col + 1) * kLdT + r]) > 0.f ? acc[c][j][1] : 0.f;
+      const float v2 = __half2float(H[col * kLdT + r + 8]) > 0.f ? acc[c][j][2] : 0.f;
+      const float v3 = __half2float(H[(col + 1) * kLdT + r + 8]) > 0.f ? acc[c][j][3] : 0.f;
+      const __half2 lo = __floats2half2_rn(v0, v1), hi = __floats2half2_rn(v2, v3);
+      *reinterpret_cast<__half2 *>(&S.G[r][col])     = lo;
+      *reinterpret_cast<__half2 *>(&S.G[r + 8][col]) = hi;
+      S.GT[col][r]         = __low2half(lo);
+      S.GT[col + 1][r]     = __high2half(lo);
+      S.GT[col][r + 8]     = __low2half(hi);
+      S.GT[col + 1][r + 8] = __high2half(hi);
+    }
+}
+
+__global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ Encoding E,
+                                                        const __half2 *__restrict__ table,
+                                                        const __half *__restrict__ w16, uint64_t n,
+                                                        const float *__restrict__ pts,
+                                                        const float *__restrict__ targets,
+                                                        float2 *__restrict__ gTable, float *__restrict__ gW,
+                                                        float *__restrict__ lossOut)
+{
+  extern __shared__ __align__(16) unsigned char smemRaw[];
+  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smemRaw);
+  loadFwdWeights(S.W, w16);
+  for (int k = threadIdx.x; k < kH * kIn; k += kThr)
+    S.w1t[k % kIn][k / kIn] = w16[kOffW1 + k];
+  for (int k = threadIdx.x; k < kH * kH; k += kThr) {
+    S.w2t[k % kH][k / kH] = w16[kOffW2 + k];
+    S.w3t[k % kH][k / kH] = w16[kOffW3 + k];
+  }
+  for (int k = threadIdx.x; k < kH; k += kThr)
+    S.w4[k] = __half2float(w16[kOffW4 + k]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  float lossAcc = 0.f;
+  for (uint64_t base = (uint64_t)blockIdx.x * kTile; base < n; base += (uint64_t)gridDim.x * kTile) {
+    const uint64_t i = base + threadIdx.x;
+    float u[3]       = {0.f, 0.f, 0.f};
+    __half2 *row     = reinterpret_cast<__half2 *>(&S.X[threadIdx.x][0]);
+    if (i < n) {
+      const f3 p = {__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2)};
+      unitPosition(E, p, u);
+      encodePoint(E, table, u, row);
+    } else {
+      for (int k = 0; k < kLv; ++k)
+        row[k] = __floats2half2_rn(0.f, 0.f);
+    }
+    S.u[threadIdx.x][0] = u[0];
+    S.u[threadIdx.x][1] = u[1];
+    S.u[threadIdx.x][2] = u[2];
+    __syncthreads();
+    for (int k = 0; k < kIn; ++k)
+      S.XT[k][threadIdx.x] = S.X[threadIdx.x][k];
+    // forward; output and d(loss)/dy per row
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int m0 = 32 * warp + 16 * c;
+      float y0, y1;
+      forwardChunk(S.W, &S.X[0][0], kIn + 8, m0, g, t, y0, y1, &S.HT[0][0][0], kLdT);
+      if (t == 0) {
+        const uint64_t r0 = base + m0 + g, r1 = r0 + 8;
+        const float d0 = r0 < n ? y0 - __ldg(targets + r0) : 0.f;
+        const float d1 = r1 < n ? y1 - __ldg(targets + r1) : 0.f;
+        S.dy[m0 + g]     = 2.f * d0;
+        S.dy[m0 + g + 8] = 2.f * d1;
+        lossAcc += d0 * d0 + d1 * d1;
+      }
+    }
+    __syncthreads();
+    // layer 4: dW4 and the signal into layer 3
+    if (threadIdx.x < kH) {
+      float s = 0.f;
+      for (int r = 0; r < kTile; ++r)
+        s += S.dy[r] * __half2float(S.HT[2][threadIdx.x][r]);
+      atomicAdd(gW + kOffW4 + threadIdx.x, s);
+    }
+    {
+      const int r = threadIdx.x;
+      for (int col = 0; col < kH; ++col) {
+        const float v = __half2float(S.HT[2][col][r]) > 0.f ? S.dy[r] * S.w4[col] : 0.f;
+        const __half h = __float2half_rn(v);
+        S.G[r][col]  = h;
+        S.GT[col][r] = h;
+      }
+    }
+    __syncthreads();
+    // layers 3 and 2: weight gradient, then the signal into the layer below
+#pragma unroll 1
+    for (int layer = 2; layer >= 1; --layer) {
+      weightGrad<8>(S, &S.HT[layer - 1][0][0], warp, g, t, gW + (layer == 2 ? kOffW3 : kOffW2), kH);
+      float acc[2][8][4];
+      signalGrad<8>(S, layer == 2 ? &S.w3t[0][0] : &S.w2t[0][0], warp, g, t, acc);
+      __syncthreads();
+      storeSignal(S, acc, &S.HT[layer - 1][0][0], warp, g, t);
+      __syncthreads();
+    }
+    // layer 1: weight gradient and the encoding gradient
+    weightGrad<4>(S, &S.XT[0][0], warp, g, t, gW + kOffW1, kIn);
+    {
+      float acc[2][4][4];
+      signalGrad<4>(S, &S.w1t[0][0], warp, g, t, acc);
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          const int r = 32 * warp + 16 * c + g + 8 * half;
+          if (base + r >= n)
+            continue;
+          const float uu[3] = {S.u[r][0], S.u[r][1], S.u[r][2]};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int l = 4 * j + t;  // columns 8j+2t, 8j+2t+1 = level l's two features
+            const float d0 = acc[c][j][2 * half], d1 = acc[c][j][2 * half + 1];
+            uint32_t ci[3];
+            float f[3];
+            levelCell(E, l, uu, ci, f);
+            float2 *gl = gTable + (size_t)l * E.tableSize;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const uint32_t e = entryOf(E, l, ci[0] + ((k >> 2) & 1), ci[1] + ((k >> 1) & 1), ci[2] + (k & 1));
+              const float w    = cornerWeight(k, f);
+              atomicAdd(gl + e, make_float2(w * d0, w * d1));
+            }
+          }
+        }
+    }
+    __syncthreads();  // shared buffers are reused by the next tile
+  }
+  // loss of this CTA
+  for (int o = 16; o > 0; o >>= 1)
+    lossAcc += __shfl_xor_sync(0xffffffffu, lossAcc, o);
+  if (lane == 0)
+    S.loss[warp] = lossAcc;
+  __syncthreads();
+  if (threadIdx.x == 0 && lossOut)
+    atomicAdd(lossOut, S.loss[0] + S.loss[1] + S.loss[2] + S.loss[3]);
+}
+
+// Adam on FP32 master parameters; refreshes the FP16 copies and clears the
+// gradient.
+__global__ void kAdam(uint64_t n, float *__restrict__ p, float *__restrict__ grad, float *__restrict__ m,
+                      float *__restrict__ v, __half *__restrict__ p16, float gradScale, float lr, float b1,
+                      float b2, float eps, float c1, float c2)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  const float gr = grad[i] * gradScale;
+  const float mi = b1 * m[i] + (1.f - b1) * gr;
+  const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+  m[i]           = mi;
+  v[i]           = vi;
+  const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  p[i]           = pi;
+  p16[i]         = __float2half_rn(pi);
+  grad[i]        = 0.f;
+}
+
+__global__ void kToHalf(uint64_t n, const float *__restrict__ p, __half *__restrict__ p16)
+{
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    p16[i] = __float2half_rn(p[i]);
+}
+
+inline unsigned blocks(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
+
+bool onDevice(const void *p)
+{
+  if (!p)
+    return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct Surrogate {
+  Device *device = nullptr;
+  Ref<Sampler> sampler;
+  Encoding E{};
+  Judge J{};
+  uint64_t tableFloats = 0;  // levels * T * 2
+  uint64_t numRegions  = 0;
+  DeviceBuffer table32, table16, w32, w16, gTable, gW, mTable, vTable, mW, vW;
+  DeviceBuffer flags, regionErr, regionSeen, scalars;
+  int step    = 0;
+  int numSMs  = 0;
+  bool dense  = false;
+
+  void zeroGrads(cudaStream_t st)
+  {
+    cudaCheck(cudaMemsetAsync(gTable.ptr, 0, tableFloats * 4, st), "memset");
+    cudaCheck(cudaMemsetAsync(gW.ptr, 0, kNumW * 4, st), "memset");
+  }
+
+  void train(uint64_t n, const float *pts, const float *targets, float *lossDev, cudaStream_t st)
+  {
+    static bool attrSet = false;
+    if (!attrSet) {
+      cudaCheck(cudaFuncSetAttribute(kSurrogateTrain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(TrainSmem)),
+                "smem attribute");
+      attrSet = true;
+    }
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, kTile), (uint64_t)numSMs * 8);
+    kSurrogateTrain<<<grid, kThr, sizeof(TrainSmem), st>>>(E, table16.as<__half2>(), w16.as<__half>(), n, pts,
+                                                           targets, gTable.as<float2>(), gW.as<float>(), lossDev);
+    cudaCheck(cudaGetLastError(), "surrogate train kernel");
+  }
+
+  void adam(uint64_t n, float lr, cudaStream_t st)
+  {
+    ++step;
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-10f;
+    const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
+    const float scale = 1.f / (float)n;
+    kAdam<<<blocks(tableFloats, 256), 256, 0, st>>>(tableFloats, table32.as<float>(), gTable.as<float>(),
+                                                    mTable.as<float>(), vTable.as<float>(), table16.as<__half>(),
+                                                    scale, lr, b1, b2, eps, c1, c2);
+    kAdam<<<blocks(kNumW, 256), 256, 0, st>>>(kNumW, w32.as<float>(), gW.as<float>(), mW.as<float>(),
+                                              vW.as<float>(), w16.as<__half>(), scale, lr, b1, b2, eps, c1, c2);
+    cudaCheck(cudaGetLastError(), "adam kernel");
+  }
+
+  template <int MODE>
+  void infer(uint64_t n, const float *pts, float *out, int fallback, cudaStream_t st)
+  {
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, kTile), (uint64_t)numSMs * 8);
+    const DevGrid &g    = sampler->volume->grid;
+    if (dense)
+      kSurrogateInfer<DenseField<float>, MODE><<<grid, kThr, 0, st>>>(E, table16.as<__half2>(), w16.as<__half>(),
+                                                                     g, J, n, pts, out, fallback);
+    else
+      kSurrogateInfer<SparseField<float>, MODE><<<grid, kThr, 0, st>>>(E, table16.as<__half2>(), w16.as<__half>(),
+                                                                      g, J, n, pts, out, fallback);
+    cudaCheck(cudaGetLastError(), "surrogate kernel");
+  }
+};
+
+}  // namespace vklcuda
+
+using namespace vklcuda;
+
+namespace {
+
+template <class F>
+VKLError surrogateCall(Surrogate *s, F &&f)
+{
+  if (!s)
+    return VKL_INVALID_ARGUMENT;
+  try {
+    f();
+    return VKL_NO_ERROR;
+  } catch (const VklError &e) {
+    s->device->setError(e.code, e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    s->device->setError(VKL_UNKNOWN_ERROR, e.what());
+    return VKL_UNKNOWN_ERROR;
+  }
+}
+
+void requireDevice(const void *p, const char *what)
+{
+  if (!onDevice(p))
+    fail(std::string("surrogate: ") + what + " must be device memory", VKL_INVALID_ARGUMENT);
+}
+
+}  // namespace
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLCudaSurrogate vklCudaNewSurrogate(VKLSampler sampler,
+                                                                      unsigned int log2TableSize,
+                                                                      float baseResolution, float growth)
+{
+  Sampler *sp = dynamic_cast<Sampler *>((ManagedObject *)sampler.host);
+  if (!sp)
+    return nullptr;
+  Device *d    = sp->device;
+  Surrogate *s = nullptr;
+  try {
+    if (!sp->volume || !sp->volume->committed)
+      fail("surrogate: the sampler's volume is not committed", VKL_INVALID_OPERATION);
+    const DevGrid &g = sp->volume->grid;
+    if (sp->s.filter != kFilterLinear || g.type[0] != kFloat || g.compress != kCompressNone)
+      fail("surrogate: needs a trilinear sampler over float voxels", VKL_INVALID_ARGUMENT);
+    if (log2TableSize < 4 || log2TableSize > 24 || !(baseResolution >= 1.f) || !(growth >= 1.f))
+      fail("surrogate: invalid hash grid configuration", VKL_INVALID_ARGUMENT);
+    s          = new Surrogate();
+    s->device  = d;
+    s->sampler = Ref<Sampler>(sp);
+    s->dense   = g.dense != 0;
+    const uint32_t T = 1u << log2TableSize;
+    s->E.tableSize   = T;
+    s->E.tableMask   = T - 1;
+    for (int l = 0; l < kLv; ++l) {
+      const float r  = std::floor(baseResolution * std::pow(growth, (float)l));
+      s->E.res[l]    = (uint32_t)std::max(1.f, r);
+      const double r1 = (double)s->E.res[l] + 1.0;
+      s->E.dense[l]  = r1 * r1 * r1 <= (double)T ? 1u : 0u;
+    }
+    const vkl_box3f &b = sp->volume->bounds;
+    const float lo[3] = {b.lower.x, b.lower.y, b.lower.z}, hi[3] = {b.upper.x, b.upper.y, b.upper.z};
+    for (int a = 0; a < 3; ++a) {
+      s->E.lo[a]      = lo[a];
+      const float ext = hi[a] - lo[a];
+      s->E.inv[a]     = 1.f / (ext > 0.f ? ext : 1.f);
+    }
+    s->tableFloats = (uint64_t)kLv * T * 2;
+    for (DeviceBuffer *buf : {&s->table32, &s->gTable, &s->mTable, &s->vTable})
+      buf->alloc(s->tableFloats * 4);
+    s->table16.alloc(s->tableFloats * 2);
+    for (DeviceBuffer *buf : {&s->w32, &s->gW, &s->mW, &s->vW})
+      buf->alloc(kNumW * 4);
+    s->w16.alloc(kNumW * 2);
+    for (DeviceBuffer *buf : {&s->table32, &s->gTable, &s->mTable, &s->vTable, &s->w32, &s->gW, &s->mW, &s->vW})
+      cudaCheck(cudaMemset(buf->ptr, 0, buf->bytes), "memset");
+    s->J.attr = 0;
+    uint64_t nr = 1;
+    for (int a = 0; a < 3; ++a) {
+      s->J.regionDims[a] = (g.activeSize[a] + (1u << kRegionLog) - 1) >> kRegionLog;
+      nr *= s->J.regionDims[a];
+    }
+    s->numRegions = nr;
+    s->flags.alloc(nr);
+    s->regionErr.alloc(nr * 4);
+    s->regionSeen.alloc(nr * 4);
+    s->scalars.alloc(16);
+    cudaCheck(cudaMemset(s->flags.ptr, 1, nr), "memset");  // everything falls back until calibrated
+    s->J.flags      = s->flags.as<uint8_t>();
+    s->J.regionErr  = s->regionErr.as<float>();
+    s->J.regionSeen = s->regionSeen.as<uint32_t>();
+    cudaCheck(cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, d->cudaDevice), "attribute");
+    return (VKLCudaSurrogate)s;
+  } catch (const VklError &e) {
+    delete s;
+    d->setError(e.code, e.what());
+  } catch (const std::exception &e) {
+    delete s;
+    d->setError(VKL_UNKNOWN_ERROR, e.what());
+  }
+  return nullptr;
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateSetParameters(VKLCudaSurrogate surrogate,
+                                                                        const float *table,
+                                                                        const float *weights)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    cudaStream_t st = s->device->stream;
+    if (table) {
+      cudaCheck(cudaMemcpyAsync(s->table32.ptr, table, s->tableFloats * 4, cudaMemcpyDefault, st), "copy");
+      kToHalf<<<blocks(s->tableFloats, 256), 256, 0, st>>>(s->tableFloats, s->table32.as<float>(),
+                                                           s->table16.as<__half>());
+    }
+    if (weights) {
+      cudaCheck(cudaMemcpyAsync(s->w32.ptr, weights, kNumW * 4, cudaMemcpyDefault, st), "copy");
+      kToHalf<<<blocks(kNumW, 256), 256, 0, st>>>(kNumW, s->w32.as<float>(), s->w16.as<__half>());
+    }
+    for (DeviceBuffer *buf : {&s->mTable, &s->vTable, &s->mW, &s->vW})
+      cudaCheck(cudaMemsetAsync(buf->ptr, 0, buf->bytes, st), "memset");
+    s->step = 0;
+    cudaCheck(cudaStreamSynchronize(st), "surrogate parameters");
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGetParameters(VKLCudaSurrogate surrogate,
+                                                                        float *table, float *weights)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    cudaStream_t st = s->device->stream;
+    if (table)
+      cudaCheck(cudaMemcpyAsync(table, s->table32.ptr, s->tableFloats * 4, cudaMemcpyDefault, st), "copy");
+    if (weights)
+      cudaCheck(cudaMemcpyAsync(weights, s->w32.ptr, kNumW * 4, cudaMemcpyDefault, st), "copy");
+    cudaCheck(cudaStreamSynchronize(st), "surrogate parameters");
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGradient(VKLCudaSurrogate surrogate, unsigned int n,
+                                                                   const vkl_vec3f *points, const float *targets,
+                                                                   float *loss, float *tableGrad,
+                                                                   float *weightGrad)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    requireDevice(points, "points");
+    requireDevice(targets, "targets");
+    cudaStream_t st = s->device->stream;
+    s->zeroGrads(st);
+    cudaCheck(cudaMemsetAsync(s->scalars.ptr, 0, 4, st), "memset");
+    s->train(n, (const float *)points, targets, s->scalars.as<float>(), st);
+    if (loss)
+      cudaCheck(cudaMemcpyAsync(loss, s->scalars.ptr, 4, cudaMemcpyDefault, st), "copy");
+    if (tableGrad)
+      cudaCheck(cudaMemcpyAsync(tableGrad, s->gTable.ptr, s->tableFloats * 4, cudaMemcpyDefault, st), "copy");
+    if (weightGrad)
+      cudaCheck(cudaMemcpyAsync(weightGrad, s->gW.ptr, kNumW * 4, cudaMemcpyDefault, st), "copy");
+    cudaCheck(cudaStreamSynchronize(st), "surrogate gradient");
+    s->zeroGrads(st);
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateTrainStep(VKLCudaSurrogate surrogate, unsigned int n,
+                                                                    const vkl_vec3f *points, const float *targets,
+                                                                    float learningRate, float *loss)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    requireDevice(points, "points");
+    requireDevice(targets, "targets");
+    if (n == 0)
+      return;
+    cudaStream_t st = s->device->stream;
+    if (loss) {
+      requireDevice(loss, "loss");
+      cudaCheck(cudaMemsetAsync(loss, 0, 4, st), "memset");
+    }
+    s->train(n, (const float *)points, targets, loss, st);
+    s->adam(n, learningRate, st);
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateCalibrate(VKLCudaSurrogate surrogate, unsigned int n,
+                                                                    const vkl_vec3f *points, float threshold,
+                                                                    unsigned int *flaggedRegions)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    requireDevice(points, "points");
+    cudaStream_t st = s->device->stream;
+    cudaCheck(cudaMemsetAsync(s->regionErr.ptr, 0, s->numRegions * 4, st), "memset");
+    cudaCheck(cudaMemsetAsync(s->regionSeen.ptr, 0, s->numRegions * 4, st), "memset");
+    cudaCheck(cudaMemsetAsync(s->scalars.ptr, 0, 4, st), "memset");
+    if (n)
+      s->infer<1>(n, (const float *)points, nullptr, 0, st);
+    kRegionFlags<<<blocks(s->numRegions, 256), 256, 0, st>>>(s->numRegions, s->regionErr.as<float>(),
+                                                             s->regionSeen.as<uint32_t>(), threshold,
+                                                             s->flags.as<uint8_t>(), s->scalars.as<unsigned int>());
+    unsigned int f = 0;
+    cudaCheck(cudaMemcpyAsync(&f, s->scalars.ptr, 4, cudaMemcpyDeviceToHost, st), "copy");
+    cudaCheck(cudaStreamSynchronize(st), "surrogate calibration");
+    if (flaggedRegions)
+      *flaggedRegions = f;
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateSample(VKLCudaSurrogate surrogate, unsigned int n,
+                                                                 const vkl_vec3f *points, float *samples,
+                                                                 int fallback)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  return surrogateCall(s, [&]() {
+    requireDevice(points, "points");
+    requireDevice(samples, "samples");
+    if (n)
+      s->infer<0>(n, (const float *)points, samples, fallback, s->device->stream);
+  });
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE void vklCudaGetSurrogateInfo(VKLCudaSurrogate surrogate, uint64_t *tableEntries,
+                                                              unsigned int *numWeights, uint64_t *numRegions,
+                                                              unsigned int *levelResolutions)
+{
+  Surrogate *s = (Surrogate *)surrogate;
+  if (!s)
+    return;
+  if (tableEntries)
+    *tableEntries = s->tableFloats / 2;
+  if (numWeights)
+    *numWeights = kNumW;
+  if (numRegions)
+    *numRegions = s->numRegions;
+  if (levelResolutions)
+    for (int l = 0; l < kLv; ++l)
+      levelResolutions[l] = s->E.res[l];
+}
+
+extern "C" OPENVKL_CUDA_INTERFACE void vklCudaReleaseSurrogate(VKLCudaSurrogate surrogate)
+{
+  delete (Surrogate *)surrogate;
+}

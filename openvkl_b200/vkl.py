@@ -66,6 +66,9 @@ EXPORTS = [
     "vklCudaGetTreeLevel", "vklCudaDenseValueRangeNoAlloc",
     "vklCudaNewSampleBatch", "vklCudaRunSampleBatch", "vklCudaGetSampleBatchConfig",
     "vklCudaReleaseSampleBatch",
+    "vklCudaNewSurrogate", "vklCudaSurrogateSetParameters", "vklCudaSurrogateGetParameters",
+    "vklCudaSurrogateGradient", "vklCudaSurrogateTrainStep", "vklCudaSurrogateCalibrate",
+    "vklCudaSurrogateSample", "vklCudaGetSurrogateInfo", "vklCudaReleaseSurrogate",
 ]
 
 
@@ -195,6 +198,15 @@ def load_library(path: str = LIB_PATH, load_only: bool = False) -> C.CDLL:
         "vklCudaRunSampleBatch": (I, [VP]),
         "vklCudaGetSampleBatchConfig": (I, [VP, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
         "vklCudaReleaseSampleBatch": (None, [VP]),
+        "vklCudaNewSurrogate": (VP, [O, U, F, F]),
+        "vklCudaSurrogateSetParameters": (I, [VP, VP, VP]),
+        "vklCudaSurrogateGetParameters": (I, [VP, VP, VP]),
+        "vklCudaSurrogateGradient": (I, [VP, U, VP, VP, VP, VP, VP]),
+        "vklCudaSurrogateTrainStep": (I, [VP, U, VP, VP, F, VP]),
+        "vklCudaSurrogateCalibrate": (I, [VP, U, VP, F, C.POINTER(U)]),
+        "vklCudaSurrogateSample": (I, [VP, U, VP, VP, I]),
+        "vklCudaGetSurrogateInfo": (None, [VP, C.POINTER(C.c_uint64), C.POINTER(U), C.POINTER(C.c_uint64), VP]),
+        "vklCudaReleaseSurrogate": (None, [VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -519,6 +531,81 @@ class SampleBatch:
     def release(self):
         if self.h:
             self.lib.vklCudaReleaseSampleBatch(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Surrogate:
+    """vklCudaNewSurrogate: hash-grid + MLP surrogate of a sampler's volume
+    (cuda device extension).  Arrays are CUDA tensors unless noted."""
+
+    LEVELS, WEIGHTS = 16, 10304
+
+    def __init__(self, sampler: "Sampler", log2_table=19, base_resolution=16.0, growth=1.5):
+        self.sampler = sampler
+        self.device = sampler.device
+        self.lib = sampler.lib
+        self.device.pending = None
+        self.h = self.lib.vklCudaNewSurrogate(sampler.h, log2_table, base_resolution, growth)
+        if not self.h:
+            self.device.raise_pending()
+            raise VKLError(*self.device.last_error())
+        entries, nw, nr = C.c_uint64(), C.c_uint(), C.c_uint64()
+        res = (C.c_uint * self.LEVELS)()
+        self.lib.vklCudaGetSurrogateInfo(self.h, C.byref(entries), C.byref(nw), C.byref(nr), res)
+        self.table_entries, self.num_weights, self.num_regions = entries.value, nw.value, nr.value
+        self.resolutions = list(res)
+
+    def _check(self, code):
+        if code != 0:
+            self.device.pending = None
+            raise VKLError(code, self.device.last_error()[1])
+
+    def set_parameters(self, table=None, weights=None):
+        t = None if table is None else np.ascontiguousarray(table, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        self._check(self.lib.vklCudaSurrogateSetParameters(self.h, None if t is None else t.ctypes.data,
+                                                           None if w is None else w.ctypes.data))
+
+    def parameters(self):
+        t = np.empty(self.table_entries * 2, np.float32)
+        w = np.empty(self.num_weights, np.float32)
+        self._check(self.lib.vklCudaSurrogateGetParameters(self.h, t.ctypes.data, w.ctypes.data))
+        return t, w
+
+    def gradient(self, points, targets):
+        t = np.empty(self.table_entries * 2, np.float32)
+        w = np.empty(self.num_weights, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self.lib.vklCudaSurrogateGradient(self.h, points.shape[0], _ptr(points), _ptr(targets),
+                                                      loss.ctypes.data, t.ctypes.data, w.ctypes.data))
+        return float(loss[0]), t, w
+
+    def train_step(self, points, targets, lr, loss=None):
+        self._check(self.lib.vklCudaSurrogateTrainStep(self.h, points.shape[0], _ptr(points), _ptr(targets),
+                                                       float(lr), _ptr(loss)))
+
+    def calibrate(self, points, threshold):
+        f = C.c_uint()
+        self._check(self.lib.vklCudaSurrogateCalibrate(self.h, points.shape[0], _ptr(points), float(threshold),
+                                                       C.byref(f)))
+        return f.value
+
+    def sample(self, points, out=None, fallback=True):
+        if out is None:
+            out = _alloc_like(points, (points.shape[0],))
+        self._check(self.lib.vklCudaSurrogateSample(self.h, points.shape[0], _ptr(points), _ptr(out),
+                                                    int(bool(fallback))))
+        return out
+
+    def release(self):
+        if self.h:
+            self.lib.vklCudaReleaseSurrogate(self.h)
             self.h = None
 
     def __del__(self):
