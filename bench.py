@@ -44,9 +44,12 @@ INCOHERENT_N = 1 << 26
 METRIC = "Gsamples/s and HBM GB/s (% roofline): plain FP32 vs FP16/FP8/batched/MLP at stated error"
 UNIT = "Gsamples/s"
 MAX_CPU_POINTS = 1 << 27  # bounded CPU sample (1.6 GB of points)
-FILTER = {"coherent": 100, "incoherent": 100, "cubic": 200, "gradient": 100, "vdb": 100, "batched": 100}
+FILTER = {"coherent": 100, "incoherent": 100, "cubic": 200, "gradient": 100, "vdb": 100, "batched": 100,
+          "intervals": 100, "hits": 100, "surrogate": 100}
 BATCH_VOLUMES = 512
 VDB_DOMAIN, VDB_POINTS = 4096, 1 << 26
+HIT_RAYS = 1 << 24
+TRAIN_STEPS = 1024
 
 
 # ---------------------------------------------------------------------------
@@ -555,6 +558,232 @@ def run_batched(args):
     del graph
 
 
+def _threaded_oracle(fn, n, threads, chunk=4096):
+    """Runs fn(start, end) over [0, n) in chunks on `threads` Python threads
+    (the oracle's ctypes calls release the GIL)."""
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda s: fn(s, min(n, s + chunk)), range(0, n, chunk)))
+
+
+def _timed_device(fn, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_intervals(args):
+    """Interval iterator on the 1024^3 volume: one iterator per pixel ray of
+    the 1920x1080 orbit camera, 4 value ranges (the quartile slices of the
+    volume's value range), default interval resolution hint, every interval
+    written out (vklIterateIntervalsN, 20 B per interval).  Unit: Mrays/s;
+    intervals per second beside it.  CPU baseline: the oracle's iterator on
+    all host threads over the first image rows."""
+    import torch
+    from openvkl_b200 import fields, vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vox = volume_numpy()
+    vol = vkl.structured_regular(dev, torch.from_numpy(vox).cuda(), shared=True)
+    smp = vkl.Sampler(vol, filter=100)
+    lo, hi = vol.value_range()
+    q = np.linspace(lo, hi, 5, dtype=np.float32)
+    vr = np.stack([q[:-1], q[1:]], 1)
+    ctx = vkl.IntervalIteratorContext(smp, value_ranges=vr)
+    o, d, t = fields.camera_rays(WIDTH, HEIGHT, (0, 0, 0), tuple(x - 1 for x in DIMS))
+    n = o.shape[0]
+    to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    go, gd, gt = to(o), to(d), to(t)
+    _, cnt = ctx.iterate_n(go, gd, gt, max_per_ray=0)
+    m = int(cnt.max().item())
+    total = int(cnt.sum().item())
+    out = torch.empty((n, m, 5), dtype=torch.float32, device="cuda")
+    cnt = torch.empty(n, dtype=torch.int32, device="cuda")
+    lib = ctx.lib
+    import ctypes as C
+    call = lambda: ctx._call(lib.vklIterateIntervalsN, C.byref(ctx.h), n, go.data_ptr(), gd.data_ptr(),
+                             gt.data_ptr(), m, out.data_ptr(), cnt.data_ptr())
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        ms = _timed_device(call, args.steps, args.warmup, stream)
+    base = None
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        ref = O.OracleVolume.dense_volume(vox, fast=True)
+        threads = os.cpu_count() or 1
+        rows = 64
+        k = rows * WIDTH
+        t0 = time.perf_counter()
+        _threaded_oracle(lambda a, b: ref.intervals(o[a:b], d[a:b], t[a:b], value_ranges=vr,
+                                                    max_intervals=m), k, threads)
+        dt = time.perf_counter() - t0
+        base = {"value": k / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                "sample": f"first {rows} image rows ({k} rays); oracle C++ restatement of the reference "
+                          f"CPU iterator, {threads} host threads, {dt:.1f} s"}
+    line = {"metric": METRIC, "value": n / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded sinusoid volume, generated rays)",
+            "config": {"workload": "interval iterator, structuredRegular 1024^3 float32, 1920x1080 orbit-camera "
+                                   "rays, 4 value ranges (quartiles), default resolution hint",
+                       "rays": n, "intervals_per_step": total, "max_per_ray": m},
+            "intervals_per_s": total / (ms * 1e-3),
+            "roofline": {"bound": "latency (per-ray serial DDA)", "alg_bytes_per_launch": n * 32 + total * 20,
+                         "achieved": (n * 32 + total * 20) / (ms * 1e-3) / 1e9, "unit": "GB/s"},
+            "cpu_baseline": base, "gpu_launches": args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_hits(args):
+    """Hit iterator on the sparse VDB (4096^3 domain shells): 2^24 random
+    rays from outside the domain towards uniform points inside it, isovalues
+    {0.25, 0.5}, trilinear filter, up to 16 hits per ray written out
+    (vklIterateHitsN, 12 B per hit).  Unit: Mrays/s."""
+    import torch
+    from openvkl_b200 import fields, vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    v, smp, origins, shells, frac = _shell_sampler(dev, VDB_DOMAIN)
+    L = origins.shape[0]
+    ctx = vkl.HitIteratorContext(smp, [0.25, 0.5])
+    n = HIT_RAYS
+    o, d, t = fields.random_rays(n, (0, 0, 0), (VDB_DOMAIN,) * 3, seed=4)
+    to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    go, gd, gt = to(o), to(d), to(t)
+    m = 16
+    out = torch.empty((n, m, 3), dtype=torch.float32, device="cuda")
+    cnt = torch.empty(n, dtype=torch.int32, device="cuda")
+    import ctypes as C
+    call = lambda: ctx._call(ctx.lib.vklIterateHitsN, C.byref(ctx.h), n, go.data_ptr(), gd.data_ptr(),
+                             gt.data_ptr(), m, out.data_ptr(), cnt.data_ptr())
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        ms = _timed_device(call, args.steps, args.warmup, stream)
+    total = int(cnt.to(torch.int64).sum().item())
+    line = {"metric": METRIC, "value": n / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded shells + fractal noise, random rays)",
+            "config": {"workload": f"hit iterator, vdb {VDB_DOMAIN}^3 domain, {L} leaves ({100 * frac:.2f} % "
+                                   f"active, {shells} shells), {n} random rays, isovalues 0.25 / 0.5",
+                       "rays": n, "hits_per_step": total, "leaves": L},
+            "hits_per_s": total / (ms * 1e-3),
+            "cpu_baseline": None, "gpu_launches": args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def _shell_sampler(dev, domain):
+    """The sparse VDB shell volume (nodesPackedDense, float leaves) and a
+    trilinear sampler over it; returns (volume, sampler, leaf origins (L,3)
+    numpy, shells, active fraction)."""
+    from openvkl_b200 import fields, vkl
+    origins, values, shells, frac = fields.shell_vdb_torch(domain=domain, seed=5)
+    L = origins.shape[0]
+    v = vkl.Volume(dev, "vdb")
+    v.set_data("node.level", vkl.Data(dev, np.full(L, 3, np.uint32)))
+    v.set_data("node.origin", vkl.Data(dev, origins.reshape(-1), vkl_type=vkl.VKL_VEC3I))
+    v.set_data("node.format", vkl.Data(dev, np.ones(L, np.uint32)))
+    v.set_data("nodesPackedDense", vkl.Data(dev, objects=[vkl.Data(dev, values, shared=True)]))
+    v.commit()
+    return v, vkl.Sampler(v, filter=100), origins, shells, frac
+
+
+def run_surrogate(args):
+    """Learned surrogate of the sparse VDB shell volume: 16-level hash grid
+    (2^19 entries per level, 2 FP16 features, base resolution 16, growth
+    1.5) + 32-64-64-64-1 ReLU MLP on FP16 tensor cores, trained with Adam
+    (lr 1e-2) on 2^28 points (2^10 steps of 2^18) whose targets the plain
+    sampler computes, half of them inside active leaves and half uniform in
+    the domain; calibrated on 2^22 points at threshold 1e-2; inference on
+    2^26 points of the same distribution against the plain sampler.  value =
+    surrogate samples/s with the plain-sampler fallback."""
+    import torch
+    from openvkl_b200 import vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vol, smp, origins, shells, frac = _shell_sampler(dev, VDB_DOMAIN)
+    sur = vkl.Surrogate(smp, log2_table=19, base_resolution=16.0, growth=1.5)
+    rng = np.random.default_rng(21)
+    table = rng.uniform(-1e-4, 1e-4, sur.table_entries * 2).astype(np.float32)
+    fan = [32, 64, 64, 64]
+    weights = np.concatenate([rng.uniform(-1, 1, 64 * fan[0]) * np.sqrt(6 / fan[0]),
+                              rng.uniform(-1, 1, 64 * 64) * np.sqrt(6 / 64),
+                              rng.uniform(-1, 1, 64 * 64) * np.sqrt(6 / 64),
+                              rng.uniform(-1, 1, 64) * np.sqrt(3 / 64)]).astype(np.float32)
+    sur.set_parameters(table, weights)
+    org = torch.from_numpy(origins).cuda().to(torch.float32)
+    g = torch.Generator(device="cuda").manual_seed(22)
+
+    def draw(n):
+        half = n // 2
+        leaf = org[torch.randint(0, org.shape[0], (half,), generator=g, device="cuda")]
+        near = leaf + torch.rand((half, 3), generator=g, device="cuda") * 8
+        uni = torch.rand((n - half, 3), generator=g, device="cuda") * VDB_DOMAIN
+        return torch.cat([near, uni]).contiguous()
+
+    steps, batch = TRAIN_STEPS, 1 << 18
+    loss = torch.zeros(1, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    train_ms, first = 0.0, None
+    for k in range(steps):
+        pts = draw(batch)
+        tgt = smp.sample(pts)
+        e0.record(stream)
+        sur.train_step(pts, tgt, 1e-2, loss)
+        e1.record(stream)
+        e1.synchronize()
+        train_ms += e0.elapsed_time(e1)
+        if k == 0:
+            first = loss.item() / batch
+    last = loss.item() / batch
+    flagged = sur.calibrate(draw(1 << 22), 1e-2)
+    n = VDB_POINTS
+    pts = draw(n)
+    out = torch.empty(n, device="cuda")
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        ms_fb = _timed_device(lambda: sur.sample(pts, out=out, fallback=True), args.steps, args.warmup, stream)
+        ms_nn = _timed_device(lambda: sur.sample(pts, out=out, fallback=False), args.steps, args.warmup, stream)
+        ms_plain = _timed_device(lambda: smp.sample(pts, out=out), args.steps, args.warmup, stream)
+    ref = smp.sample(pts)
+    vrange = float(vol.value_range()[1] - vol.value_range()[0])
+
+    def err(fb):
+        e = (sur.sample(pts, fallback=fb) - ref).abs()
+        return {"max_abs": float(e.max().item()), "mean_abs": float(e.mean().item()),
+                "frac_above_1e-2": float((e > 1e-2).float().mean().item())}
+
+    rate = lambda ms: n / (ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": rate(ms_fb), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_fb, "higher_is_better": True, "dtype": "fp16 (MLP), f32",
+            "data": "synthetic (seeded shells + fractal noise)",
+            "config": {"workload": f"surrogate of vdb {VDB_DOMAIN}^3 domain ({origins.shape[0]} leaves, "
+                                   f"{shells} shells): hash grid 16 x 2^19 x 2 fp16, MLP 32-64-64-64-1; "
+                                   f"{n} inference points, half in active leaves",
+                       "train_points": steps * batch, "value_range": vrange},
+            "surrogate_no_fallback": {"value": rate(ms_nn), "ms_per_step": ms_nn},
+            "plain": {"value": rate(ms_plain), "ms_per_step": ms_plain},
+            "train": {"points_per_s": steps * batch / (train_ms * 1e-3), "ms_total": train_ms,
+                      "loss_first": first, "loss_last": last},
+            "calibration": {"threshold": 1e-2, "flagged_regions": flagged, "regions": sur.num_regions},
+            "error_vs_plain": {"fallback": err(True), "no_fallback": err(False)},
+            "gpu_launches": 3 * args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    sur.release()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -570,9 +799,10 @@ def main(argv=None):
                          "the ncu capture case")
     args = ap.parse_args(argv)
     if args.small:
-        global DIMS, WIDTH, HEIGHT, INCOHERENT_N, VDB_DOMAIN, VDB_POINTS
+        global DIMS, WIDTH, HEIGHT, INCOHERENT_N, VDB_DOMAIN, VDB_POINTS, HIT_RAYS
         DIMS, WIDTH, HEIGHT, INCOHERENT_N = (512, 512, 512), 480, 270, 1 << 24
-        VDB_DOMAIN, VDB_POINTS = 2048, 1 << 24
+        global TRAIN_STEPS
+        VDB_DOMAIN, VDB_POINTS, HIT_RAYS, TRAIN_STEPS = 2048, 1 << 24, 1 << 20, 64
     if args.no_extras:
         args.no_cpu_baseline = True
     if args.impl == "reference":
@@ -581,6 +811,12 @@ def main(argv=None):
         run_vdb(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "intervals":
+        run_intervals(args)
+    elif args.workload == "hits":
+        run_hits(args)
+    elif args.workload == "surrogate":
+        run_surrogate(args)
     else:
         run_cuda(args)
 

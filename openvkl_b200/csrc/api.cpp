@@ -4,6 +4,7 @@
 // converts exceptions into the device's last error plus error callback,
 // returning the reference's sentinel values (NaN sample, null handle, 0)
 // (openvkl/api/API.cpp:37-89, devices/cpu/api/DeviceAPI.cpp:25-57).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -95,35 +96,96 @@ Sampler *committedSampler(const VKLSampler *s)
   return sp;
 }
 
-// Runs `launch(devIn, devOut)` on the device stream with inputs / outputs
-// that may be host or device memory; host arrays are staged and the call
-// synchronizes before returning.
+// Points per chunk of a pipelined host-pointer call (a multiple of the
+// sampling kernels' 2048-point tile, so every chunk starts 16-byte aligned).
+constexpr uint64_t kPipeChunk = uint64_t(1) << 23;
+// Host-pointer calls below this many input bytes are staged in one piece.
+constexpr size_t kPipeMinBytes = size_t(32) << 20;
+
+// Runs `launch(n, devIn, devOut)` over N independent items (inStride /
+// outStride bytes each) on the device stream, with inputs / outputs that
+// may be host or device memory.  Host arrays are staged through device
+// buffers and the call synchronizes before returning; large host-pointer
+// calls are cut into chunks whose copies overlap the kernels of their
+// neighbours (copy streams ordered against the device stream by events).
 template <class Launch>
-void staged(Device *d, const void *in, size_t inBytes, void *out, size_t outBytes,
+void staged(Device *d, uint64_t N, size_t inStride, const void *in, size_t outStride, void *out,
             Launch &&launch)
 {
   const bool inDev = isDevicePtr(in), outDev = isDevicePtr(out);
   if (inDev && outDev) {
-    launch(in, out);
+    launch(N, in, out);
     return;
   }
   std::lock_guard<std::mutex> lock(d->stagingMutex);
-  const void *din = in;
-  void *dout      = out;
-  if (!inDev) {
-    d->stageIn.reserve(inBytes);
-    cudaCheck(cudaMemcpyAsync(d->stageIn.ptr, in, inBytes, cudaMemcpyHostToDevice, d->stream),
-              "stage in");
-    din = d->stageIn.ptr;
+  if (N * inStride < kPipeMinBytes) {
+    const void *din = in;
+    void *dout      = out;
+    if (!inDev) {
+      d->stageIn.reserve(N * inStride);
+      cudaCheck(cudaMemcpyAsync(d->stageIn.ptr, in, N * inStride, cudaMemcpyHostToDevice,
+                                d->stream),
+                "stage in");
+      din = d->stageIn.ptr;
+    }
+    if (!outDev) {
+      d->stageOut.reserve(N * outStride);
+      dout = d->stageOut.ptr;
+    }
+    launch(N, din, dout);
+    if (!outDev)
+      cudaCheck(cudaMemcpyAsync(out, dout, N * outStride, cudaMemcpyDeviceToHost, d->stream),
+                "stage out");
+    cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
+    return;
   }
-  if (!outDev) {
-    d->stageOut.reserve(outBytes);
-    dout = d->stageOut.ptr;
-  }
-  launch(din, dout);
+
+  // Chunk k uses slot k % S: its input copy waits for the kernel of chunk
+  // k - S (which read the slot), its kernel for that chunk's output copy.
+  constexpr int S = Device::kPipeSlots;
+  d->ensurePipeline();
+  const uint64_t C = kPipeChunk;
+  if (!inDev)
+    d->stageIn.reserve(S * C * inStride);
   if (!outDev)
-    cudaCheck(cudaMemcpyAsync(out, dout, outBytes, cudaMemcpyDeviceToHost, d->stream),
-              "stage out");
+    d->stageOut.reserve(S * C * outStride);
+  cudaCheck(cudaEventRecord(d->pipeStart, d->stream), "pipeline");
+  cudaCheck(cudaStreamWaitEvent(d->copyIn, d->pipeStart, 0), "pipeline");
+  cudaCheck(cudaStreamWaitEvent(d->copyOut, d->pipeStart, 0), "pipeline");
+  const uint64_t K = (N + C - 1) / C;
+  for (uint64_t k = 0; k < K; ++k) {
+    const int s        = int(k % S);
+    const uint64_t off = k * C, n = std::min(C, N - off);
+    const void *din    = (const uint8_t *)in + off * inStride;
+    void *dout         = (uint8_t *)out + off * outStride;
+    if (!inDev) {
+      void *slot = (uint8_t *)d->stageIn.ptr + s * C * inStride;
+      if (k >= (uint64_t)S)
+        cudaCheck(cudaStreamWaitEvent(d->copyIn, d->computed[s], 0), "pipeline");
+      cudaCheck(cudaMemcpyAsync(slot, din, n * inStride, cudaMemcpyHostToDevice, d->copyIn),
+                "stage in");
+      cudaCheck(cudaEventRecord(d->inReady[s], d->copyIn), "pipeline");
+      cudaCheck(cudaStreamWaitEvent(d->stream, d->inReady[s], 0), "pipeline");
+      din = slot;
+    }
+    void *hostOut = dout;
+    if (!outDev) {
+      if (k >= (uint64_t)S)
+        cudaCheck(cudaStreamWaitEvent(d->stream, d->drained[s], 0), "pipeline");
+      dout = (uint8_t *)d->stageOut.ptr + s * C * outStride;
+    }
+    launch(n, din, dout);
+    cudaCheck(cudaEventRecord(d->computed[s], d->stream), "pipeline");
+    if (!outDev) {
+      cudaCheck(cudaStreamWaitEvent(d->copyOut, d->computed[s], 0), "pipeline");
+      cudaCheck(cudaMemcpyAsync(hostOut, dout, n * outStride, cudaMemcpyDeviceToHost, d->copyOut),
+                "stage out");
+      cudaCheck(cudaEventRecord(d->drained[s], d->copyOut), "pipeline");
+    }
+  }
+  // the device stream resumes after the last copies (and the call returns then)
+  if (!outDev)
+    cudaCheck(cudaStreamWaitEvent(d->stream, d->drained[(K - 1) % S], 0), "pipeline");
   cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
 }
 
@@ -141,8 +203,8 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
   if (!pts || !out)
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
-  staged(d, pts, N * 12, out, N * 4 * M, [&](const void *din, void *dout) {
-    launchSample(s->volume->grid, s->s.filter, s->s.maxSamplingDepth, N, (const float *)din, M,
+  staged(d, N, 12, pts, 4 * M, out, [&](uint64_t n, const void *din, void *dout) {
+    launchSample(s->volume->grid, s->s.filter, s->s.maxSamplingDepth, n, (const float *)din, M,
                  attrs, (float *)dout, d->stream);
   });
 }
@@ -158,8 +220,8 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
   if (!pts || !out)
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
-  staged(d, pts, N * 12, out, N * 12, [&](const void *din, void *dout) {
-    launchGradient(s->volume->grid, s->s.gradientFilter, s->s.maxSamplingDepth, N,
+  staged(d, N, 12, pts, 12, out, [&](uint64_t n, const void *din, void *dout) {
+    launchGradient(s->volume->grid, s->s.gradientFilter, s->s.maxSamplingDepth, n,
                    (const float *)din, attr, (float *)dout, d->stream);
   });
 }

@@ -181,6 +181,36 @@ Data *ManagedObject::getData(const std::string &name) const
 // ---------------------------------------------------------------------------
 // Device.
 // ---------------------------------------------------------------------------
+void Device::ensurePipeline()
+{
+  if (copyIn)
+    return;
+  cudaCheck(cudaStreamCreateWithFlags(&copyIn, cudaStreamNonBlocking), "copy stream");
+  cudaCheck(cudaStreamCreateWithFlags(&copyOut, cudaStreamNonBlocking), "copy stream");
+  cudaCheck(cudaEventCreateWithFlags(&pipeStart, cudaEventDisableTiming), "copy event");
+  for (int s = 0; s < kPipeSlots; ++s) {
+    cudaCheck(cudaEventCreateWithFlags(&inReady[s], cudaEventDisableTiming), "copy event");
+    cudaCheck(cudaEventCreateWithFlags(&computed[s], cudaEventDisableTiming), "copy event");
+    cudaCheck(cudaEventCreateWithFlags(&drained[s], cudaEventDisableTiming), "copy event");
+  }
+}
+
+Device::~Device()
+{
+  if (!copyIn)
+    return;
+  cudaStreamSynchronize(copyIn);
+  cudaStreamSynchronize(copyOut);
+  for (int s = 0; s < kPipeSlots; ++s) {
+    cudaEventDestroy(inReady[s]);
+    cudaEventDestroy(computed[s]);
+    cudaEventDestroy(drained[s]);
+  }
+  cudaEventDestroy(pipeStart);
+  cudaStreamDestroy(copyIn);
+  cudaStreamDestroy(copyOut);
+}
+
 void Device::setError(VKLError code, const std::string &msg)
 {
   lastErrorCode = code;

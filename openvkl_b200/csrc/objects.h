@@ -176,6 +176,17 @@ struct Device {
   std::mutex stagingMutex;
   DeviceBuffer stageIn, stageOut, stageAux;
 
+  // Chunked host-pointer calls overlap the host->device copy of chunk k+1
+  // and the device->host copy of chunk k-1 with the kernel on chunk k:
+  // copies run on two streams of their own, ordered against `stream` by
+  // events, through kPipeSlots staging slots.  Created on first use.
+  static constexpr int kPipeSlots = 3;
+  cudaStream_t copyIn = nullptr, copyOut = nullptr;
+  cudaEvent_t pipeStart = nullptr;
+  cudaEvent_t inReady[kPipeSlots]{}, computed[kPipeSlots]{}, drained[kPipeSlots]{};
+  void ensurePipeline();
+  ~Device();
+
   void setError(VKLError code, const std::string &msg);
   void log(int level, const std::string &msg);
 };

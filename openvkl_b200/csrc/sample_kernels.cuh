@@ -78,11 +78,11 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
 {
   constexpr int PPT  = TILE / kTileThreads;
   constexpr int OUTF = GRAD ? 3 : 1;
-  // sx | sy | sz; before the sort the same words hold the tile's points as
-  // the caller laid them out (x, y, z per point)
-  __shared__ __align__(16) float sxyz[3 * TILE];
-  float *const sx = sxyz, *const sy = sxyz + TILE, *const sz = sxyz + 2 * TILE;
-  __shared__ uint16_t sidx[TILE];
+  // Before the sort these words hold the tile's points as the caller laid
+  // them out (x, y, z per point); after it, spt[k] = the k-th point in
+  // brick order (index space) with its position in the tile as w.
+  __shared__ __align__(16) float4 spt[TILE];
+  float *const sxyz = reinterpret_cast<float *>(spt);
   __shared__ float res[TILE * OUTF];
   __shared__ __align__(16) int hist[kSortBins];
   const uint64_t base = (uint64_t)blockIdx.x * TILE;
@@ -105,22 +105,24 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
       sxyz[k] = __ldcs(src + k);
   }
   f3 p[PPT];
-  uint32_t key[PPT];
+  uint32_t slot[PPT];  // bin (low 10 bits) | rank within the bin (high bits)
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < PPT; ++j) {
     const int k = threadIdx.x + j * kTileThreads;
     if (k < cnt) {
-      p[j]   = xfmPoint(g.objectToIndex, f3{sxyz[3 * k], sxyz[3 * k + 1], sxyz[3 * k + 2]});
-      key[j] = tileKey(p[j]);
-      atomicAdd(&hist[key[j]], 1);
+      p[j]             = xfmPoint(g.objectToIndex, f3{sxyz[3 * k], sxyz[3 * k + 1], sxyz[3 * k + 2]});
+      const uint32_t b = tileKey(p[j]);
+      slot[j]          = b | ((uint32_t)atomicAdd(&hist[b], 1) << 10);
     }
   }
+  // after this barrier no thread reads the raw points again, so the scatter
+  // may overwrite them
   __syncthreads();
   {
     // exclusive scan of the histogram: 4 bins per thread, warp scans, then
     // the warp totals
-    static_assert(kSortBins == 4 * kTileThreads, "scan layout");
+    static_assert(kSortBins == 4 * kTileThreads && kSortBins == 1024, "scan layout");
     __shared__ int warpSum[kTileThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int4 h   = reinterpret_cast<const int4 *>(hist)[threadIdx.x];
@@ -146,11 +148,8 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
   for (int j = 0; j < PPT; ++j) {
     const int k = threadIdx.x + j * kTileThreads;
     if (k < cnt) {
-      const int pos = atomicAdd(&hist[key[j]], 1);
-      sx[pos]       = p[j].x;
-      sy[pos]       = p[j].y;
-      sz[pos]       = p[j].z;
-      sidx[pos]     = (uint16_t)k;
+      const int pos = hist[slot[j] & (kSortBins - 1)] + (int)(slot[j] >> 10);
+      spt[pos]      = make_float4(p[j].x, p[j].y, p[j].z, __int_as_float(k));
     }
   }
   __syncthreads();
@@ -161,8 +160,9 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
   auto compute = [&](int j) {
     const int k = threadIdx.x + j * kTileThreads;
     if (k < cnt) {
-      const f3 q = {sx[k], sy[k], sz[k]};
-      const int o = sidx[k];
+      const float4 e = spt[k];
+      const f3 q     = {e.x, e.y, e.z};
+      const int o    = __float_as_int(e.w);
       if (GRAD) {
         f3 r = {0.f, 0.f, 0.f};
         if (FILTER != kFilterNearest) {
@@ -197,7 +197,7 @@ template <typename T, bool DENSE, int FILTER>
 void launchTyped(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float *pts, uint32_t attr,
                  float *out, bool grad, cudaStream_t st)
 {
-  // 2048-point tiles for samples (40 KB shared), 1024 for gradients and the
+  // 2048-point tiles for samples (44 KB shared), 1024 for gradients and the
   // register-heavy tricubic.
   if (grad) {
     constexpr int TILE = 1024;

@@ -49,7 +49,10 @@ def build(fast: bool = True) -> None:
     """Compile the parity build with the committed Makefile and, if asked,
     the -march=native timing build for this host."""
     subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle.so"], check=True)
-    if fast and not os.path.exists(fast_path()):
+    srcs = [os.path.join(_HERE, f) for f in ("vkl_oracle.cpp", "vkl_oracle.h")]
+    stale = not os.path.exists(fast_path()) or \
+        os.path.getmtime(fast_path()) < max(os.path.getmtime(f) for f in srcs)
+    if fast and stale:
         subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle_fast.so"], check=True)
         os.replace(os.path.join(_BUILD, "liboracle_fast.so"), fast_path())
 
@@ -61,8 +64,7 @@ def lib(fast: bool = False) -> C.CDLL:
     name = fast_path() if fast else os.path.join(_BUILD, "liboracle.so")
     if name not in _libs:
         path = name
-        if not os.path.exists(path):
-            build(fast=fast)
+        build(fast=fast)
         L = C.CDLL(path)
         P, U32, U64, I32, F32, VP = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float, C.c_void_p
         L.orc_dense_create.restype = P
