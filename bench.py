@@ -682,10 +682,11 @@ def run_hits(args):
     print(json.dumps(line), flush=True)
 
 
-def _shell_sampler(dev, domain):
+def _shell_sampler(dev, domain, background=None):
     """The sparse VDB shell volume (nodesPackedDense, float leaves) and a
     trilinear sampler over it; returns (volume, sampler, leaf origins (L,3)
-    numpy, shells, active fraction)."""
+    numpy, shells, active fraction).  Without `background` the volume keeps
+    the reference's undefined (NaN) background."""
     from openvkl_b200 import fields, vkl
     origins, values, shells, frac = fields.shell_vdb_torch(domain=domain, seed=5)
     L = origins.shape[0]
@@ -694,6 +695,8 @@ def _shell_sampler(dev, domain):
     v.set_data("node.origin", vkl.Data(dev, origins.reshape(-1), vkl_type=vkl.VKL_VEC3I))
     v.set_data("node.format", vkl.Data(dev, np.ones(L, np.uint32)))
     v.set_data("nodesPackedDense", vkl.Data(dev, objects=[vkl.Data(dev, values, shared=True)]))
+    if background is not None:
+        v.set_data("background", vkl.Data(dev, np.asarray([background], np.float32)))
     v.commit()
     return v, vkl.Sampler(v, filter=100), origins, shells, frac
 
@@ -713,7 +716,9 @@ def run_surrogate(args):
     dev = vkl.Device("cuda")
     stream = torch.cuda.current_stream()
     dev.set_stream(stream.cuda_stream)
-    vol, smp, origins, shells, frac = _shell_sampler(dev, VDB_DOMAIN)
+    # a fog volume: empty space has density 0 (the reference's undefined
+    # background would make every sample outside the leaves NaN)
+    vol, smp, origins, shells, frac = _shell_sampler(dev, VDB_DOMAIN, background=0.0)
     sur = vkl.Surrogate(smp, log2_table=19, base_resolution=16.0, growth=1.5)
     rng = np.random.default_rng(21)
     table = rng.uniform(-1e-4, 1e-4, sur.table_entries * 2).astype(np.float32)

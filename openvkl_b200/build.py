@@ -28,7 +28,8 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,
          "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 
 SOURCES = ["api.cpp", "objects.cpp", "k_sample.cu", "k_sample_nearest.cu", "k_sample_linear.cu",
-           "k_sample_cubic.cu", "k_build.cu", "k_iterate.cu", "k_noalloc.cu", "k_batch.cu", "k_surrogate.cu"]
+           "k_sample_cubic.cu", "k_build.cu", "k_iterate.cu", "k_noalloc.cu", "k_batch.cu", "k_surrogate.cu",
+           "k_bin.cu"]
 
 
 def _headers():

@@ -189,6 +189,22 @@ void staged(Device *d, uint64_t N, size_t inStride, const void *in, size_t outSt
   cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
 }
 
+// Incoherent large calls on dense float volumes go through binned sampling
+// (k_bin.cu); returns false where the ordinary launch is to run.
+bool binned(Device *d, Sampler *s, int filter, uint64_t n, const float *pts, uint32_t attr, float *out,
+            bool grad)
+{
+  const DevGrid &g = s->volume->grid;
+  if (!d->binning || !binnedSamplingApplies(g, filter, n, attr))
+    return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaCheck(cudaStreamIsCapturing(d->stream, &cs), "capture status");
+  if (cs != cudaStreamCaptureStatusNone)  // the coherence test reads back a count
+    return false;
+  std::lock_guard<std::mutex> lock(d->binMutex);
+  return launchSampleBinned(g, filter, n, pts, attr, out, grad, d->binScratch, d->stream);
+}
+
 void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float *out,
              uint32_t M, const uint32_t *attrs)
 {
@@ -204,6 +220,8 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
   staged(d, N, 12, pts, 4 * M, out, [&](uint64_t n, const void *din, void *dout) {
+    if (M == 1 && binned(d, s, s->s.filter, n, (const float *)din, attrs[0], (float *)dout, false))
+      return;
     launchSample(s->volume->grid, s->s.filter, s->s.maxSamplingDepth, n, (const float *)din, M,
                  attrs, (float *)dout, d->stream);
   });
@@ -221,6 +239,8 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
   staged(d, N, 12, pts, 12, out, [&](uint64_t n, const void *din, void *dout) {
+    if (binned(d, s, s->s.gradientFilter, n, (const float *)din, attr, (float *)dout, true))
+      return;
     launchGradient(s->volume->grid, s->s.gradientFilter, s->s.maxSamplingDepth, n,
                    (const float *)din, attr, (float *)dout, d->stream);
   });
@@ -326,6 +346,8 @@ void vklDeviceSetInt(VKLDevice dev, const char *name, int x)
   d->intParams[name] = x;
   if (!std::strcmp(name, "logLevel"))
     d->logLevel = x;
+  if (!std::strcmp(name, "binnedSampling"))
+    d->binning = x != 0;
 }
 
 void vklDeviceSetString(VKLDevice dev, const char *name, const char *s)

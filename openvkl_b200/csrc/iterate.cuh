@@ -223,6 +223,12 @@ struct IntervalIt {
   float nominalDeltaT;
   uint32_t budget;
   Dda dda;
+  // The last sparse query that ended on a leaf pointer of level 2 at full
+  // depth: every elementary cell of that leaf gets the same descriptor (the
+  // walk reads the same three node voxels), so the next cells reuse it.
+  int32_t leafKey[3];
+  bool leafKeyValid;
+  VoxelDesc leafDesc;
 };
 
 // intersectBox (math/box_utility.ih:63-77)
@@ -254,13 +260,34 @@ __device__ inline void intervalInit(const DevGrid &g, uint32_t depth, f3 origin,
                           1.f * divideSafe(fabsf(dir.z)));
   float lo, hi;
   intersectBox(org, dir, g.domain, tLo, tHi, lo, hi);
-  it.budget = kMaxDdaSteps;
+  it.budget       = kMaxDdaSteps;
+  it.leafKeyValid = false;
   if (hi <= lo) {
     it.tMax  = -kPosInf;
     it.dda.t = 0.f;
   } else {
     it.tMax = hi;
     ddaInit(org, dir, lo, depth, it.dda);
+  }
+}
+
+__device__ __forceinline__ void querySparseCached(const DevGrid &g, int32_t x, int32_t y, int32_t z,
+                                                  uint32_t depth, uint32_t attr, const DevValueRanges &vr,
+                                                  IntervalIt &it, VoxelDesc &desc)
+{
+  const bool full = depth >= kNumLevels - 1;
+  if (full && it.leafKeyValid && (x >> 3) == it.leafKey[0] && (y >> 3) == it.leafKey[1] &&
+      (z >> 3) == it.leafKey[2]) {
+    desc = it.leafDesc;
+    return;
+  }
+  queryVoxelSparse(g, x, y, z, depth, attr, vr, desc);
+  if (full && desc.level == kNumLevels - 1) {
+    it.leafKeyValid = true;
+    it.leafKey[0]   = x >> 3;
+    it.leafKey[1]   = y >> 3;
+    it.leafKey[2]   = z >> 3;
+    it.leafDesc     = desc;
   }
 }
 
@@ -275,7 +302,7 @@ __device__ inline bool intervalNext(const DevGrid &g, uint32_t attr, const DevVa
     if (g.dense)
       queryVoxelDense(g, it.dda.idx[L], it.dda.idx[4 + L], it.dda.idx[8 + L], L, attr, vr, desc);
     else
-      queryVoxelSparse(g, it.dda.idx[L], it.dda.idx[4 + L], it.dda.idx[8 + L], L, attr, vr, desc);
+      querySparseCached(g, it.dda.idx[L], it.dda.idx[4 + L], it.dda.idx[8 + L], L, attr, vr, it, desc);
     if (!desc.isEmpty)
       break;
     if (it.budget-- == 0) {
@@ -311,20 +338,43 @@ __device__ __noinline__ float hitSample(const DevGrid &g, int filter, uint32_t a
   return sampleObjectAny(g, filter, attr, depth, p);
 }
 
-struct HitCtx {
+// Sample hooks of the hit iterator's marching.  AnySampleHook dispatches on
+// the volume's voxel type and filter out of line (one copy shared by every
+// call site: the per-ray C API and the generic batched kernel); the
+// specialised LinearSampleHook inlines one field type with the trilinear
+// filter.  Both evaluate exactly sampleObjectAny's expression.
+struct AnySampleHook {
   const DevGrid *g;
   int filter;
   uint32_t attr;
   uint32_t depth;
-  f3 o, d;
-  __device__ __forceinline__ float sampleAt(float t) const
+  __device__ __forceinline__ float operator()(f3 oc) const { return hitSample(*g, filter, attr, depth, oc); }
+};
+
+template <class Field>
+struct LinearSampleHook {
+  const DevGrid *g;
+  Field F;
+  __device__ __forceinline__ float operator()(f3 oc) const
   {
-    return hitSample(*g, filter, attr, depth, {o.x + t * d.x, o.y + t * d.y, o.z + t * d.z});
+    return sampleLinear(F, xfmPoint(g->objectToIndex, oc));
   }
 };
 
-__device__ inline float bisect(const HitCtx &c, float t0, float s0, float t, float s, float iso,
-                               float tol)
+template <class Hook>
+struct HitCtx {
+  Hook sample;
+  f3 o, d;
+  __device__ __forceinline__ float sampleAt(float t) const
+  {
+    return sample({o.x + t * d.x, o.y + t * d.y, o.z + t * d.z});
+  }
+};
+
+// bisect (Iterator.ih): at most 10 halvings of [t0, t] towards the iso
+// crossing.
+template <class Ctx>
+__device__ inline float bisect(const Ctx &c, float t0, float s0, float t, float s, float iso, float tol)
 {
   int iter   = 0;
   float tMid = 0.f;
@@ -350,57 +400,93 @@ __device__ inline float bisect(const HitCtx &c, float t0, float s0, float t, flo
   return tMid;
 }
 
-__device__ inline bool intersectBisection(const HitCtx &c, float tLo, float tHi, float step,
-                                          uint32_t numValues, const float *values, DevHit &hit)
+// intersectSurfacesBisection (Iterator.ih): march [tLo, tHi) with the
+// interval's nominal step, find the first iso crossing, refine it by
+// bisection.  With LOOKAHEAD > 1 the t of the next LOOKAHEAD march steps
+// are computed first (the same serial additions) and their samples issued
+// together, so their loads overlap; the steps are then examined in order
+// exactly as the one-step loop would, and samples past a hit are discarded.
+//
+// (cacheT, cacheS) is the last march sample of the ray, (t, sampleAt(t)): an
+// interval that starts where the previous one's march ended (the usual case:
+// the DDA's intervals abut and the march's last step lands on the interval
+// end) reuses it instead of sampling the same t again.
+template <int LOOKAHEAD, class Ctx>
+__device__ inline bool intersectBisection(const Ctx &c, float tLo, float tHi, float step, uint32_t numValues,
+                                          const float *values, DevHit &hit, float &cacheT, float &cacheS)
 {
   float t0 = tLo;
-  float s0 = c.sampleAt(t0);
+  float s0 = t0 == cacheT ? cacheS : c.sampleAt(t0);
   for (int it = 0; (float)it < 10.f && isnan(s0) && t0 < tHi; ++it) {
     t0 += maxx(1e-5f, 1e-5f * step);
     s0 = c.sampleAt(t0);
   }
-  for (uint32_t march = 0; t0 < tHi && march < kMaxMarchSteps; ++march) {
-    const float h = minx(step, tHi - t0);
-    const float t = t0 + h;
-    float s       = c.sampleAt(t);
-    float ts      = t;
-    for (int it = 0; (float)it < 10.f && isnan(s) && ts > t0; ++it) {
-      ts -= maxx(1e-5f, 1e-5f * step);
-      s = c.sampleAt(ts);
-    }
-    float tHit = kPosInf, eps = kPosInf, value = kPosInf;
-    for (uint32_t i = 0; i < numValues; ++i) {
-      const float vi = __ldg(values + i);
-      if (fabsf(s0 - vi) < 1e-6f) {
-        if (t0 < tHit && t0 <= tHi) {
-          tHit  = t0;
-          value = vi;
-          eps   = 0.125f * step;
+  uint32_t march = 0;
+  while (t0 < tHi && march < kMaxMarchSteps) {
+    float tk[LOOKAHEAD], hk[LOOKAHEAD], sk[LOOKAHEAD];
+    int kn   = 0;
+    float tt = t0;
+#pragma unroll
+    for (int k = 0; k < LOOKAHEAD; ++k)
+      if (tt < tHi && march + (uint32_t)k < kMaxMarchSteps) {
+        hk[k] = minx(step, tHi - tt);
+        tk[k] = tt + hk[k];
+        tt    = tk[k];
+        kn    = k + 1;
+      }
+#pragma unroll
+    for (int k = 0; k < LOOKAHEAD; ++k)
+      if (k < kn)
+        sk[k] = c.sampleAt(tk[k]);
+    cacheT = tk[kn - 1];
+    cacheS = sk[kn - 1];
+#pragma unroll
+    for (int k = 0; k < LOOKAHEAD; ++k) {
+      if (k >= kn)
+        break;
+      const float h = hk[k];
+      const float t = tk[k];
+      float s       = sk[k];
+      float ts      = t;
+      for (int it = 0; (float)it < 10.f && isnan(s) && ts > t0; ++it) {
+        ts -= maxx(1e-5f, 1e-5f * step);
+        s = c.sampleAt(ts);
+      }
+      float tHit = kPosInf, eps = kPosInf, value = kPosInf;
+      for (uint32_t i = 0; i < numValues; ++i) {
+        const float vi = __ldg(values + i);
+        if (fabsf(s0 - vi) < 1e-6f) {
+          if (t0 < tHit && t0 <= tHi) {
+            tHit  = t0;
+            value = vi;
+            eps   = 0.125f * step;
+          }
+        } else if (!isnan(s0 + s) && (vi - s0) * (vi - s) < 0.f) {
+          const float tIso = bisect(c, t0, s0, ts, s, vi, minx(1e-6f, 0.01f * h));
+          if (tIso < tHit && tIso <= tHi) {
+            tHit  = tIso;
+            value = vi;
+            eps   = 0.125f * step;
+          }
         }
-      } else if (!isnan(s0 + s) && (vi - s0) * (vi - s) < 0.f) {
-        const float tIso = bisect(c, t0, s0, ts, s, vi, minx(1e-6f, 0.01f * h));
-        if (tIso < tHit && tIso <= tHi) {
-          tHit  = tIso;
-          value = vi;
-          eps   = 0.125f * step;
+        if (t == tHi && fabsf(s - vi) < 1e-6f) {
+          if (ts < tHit && ts <= tHi) {
+            tHit  = ts;
+            value = vi;
+            eps   = 0.125f * step;
+          }
         }
       }
-      if (t == tHi && fabsf(s - vi) < 1e-6f) {
-        if (ts < tHit && ts <= tHi) {
-          tHit  = ts;
-          value = vi;
-          eps   = 0.125f * step;
-        }
+      if (tHit < kPosInf) {
+        hit.t       = tHit;
+        hit.sample  = value;
+        hit.epsilon = eps * sqrtf(c.d.x * c.d.x + c.d.y * c.d.y + c.d.z * c.d.z);
+        return true;
       }
+      t0 = t;
+      s0 = s;
     }
-    if (tHit < kPosInf) {
-      hit.t       = tHit;
-      hit.sample  = value;
-      hit.epsilon = eps * sqrtf(c.d.x * c.d.x + c.d.y * c.d.y + c.d.z * c.d.z);
-      return true;
-    }
-    t0 = t;
-    s0 = s;
+    march += (uint32_t)kn;
   }
   return false;
 }
@@ -411,6 +497,7 @@ struct HitIt {
   f3 o, d;
   DevInterval cur;
   float lastHitOffsetT;
+  float cacheT, cacheS;  // last march sample (intersectBisection)
 };
 
 __device__ inline void hitInit(const DevGrid &g, uint32_t depth, f3 o, f3 d, float tLo, float tHi,
@@ -421,18 +508,20 @@ __device__ inline void hitInit(const DevGrid &g, uint32_t depth, f3 o, f3 d, flo
   h.d              = d;
   h.cur            = {1.f, -1.f, 0.f, 0.f, 0.f};
   h.lastHitOffsetT = -kPosInf;
+  h.cacheT         = __builtin_nanf("");
+  h.cacheS         = 0.f;
 }
 
 // One vklIterateHit call (DefaultIterator.ispc:168-258).
-__device__ inline bool hitNext(const DevGrid &g, int filter, uint32_t attr, uint32_t sampleDepth,
-                               const DevValueRanges &vr, uint32_t numValues, const float *values,
-                               HitIt &h, DevHit &hit)
+template <int LOOKAHEAD, class Hook>
+__device__ inline bool hitNextWith(const DevGrid &g, const Hook &hook, uint32_t attr, const DevValueRanges &vr,
+                                   uint32_t numValues, const float *values, HitIt &h, DevHit &hit)
 {
   if (numValues == 0)
     return false;
   if (h.cur.t0 == kPosInf)
     return false;
-  const HitCtx c{&g, filter, attr, sampleDepth, h.o, h.d};
+  const HitCtx<Hook> c{hook, h.o, h.d};
   for (;;) {
     const bool need = h.cur.t1 <= h.cur.t0;
     bool have       = !need;
@@ -448,13 +537,271 @@ __device__ inline bool hitNext(const DevGrid &g, int filter, uint32_t attr, uint
       return false;
     }
     hit.t = kPosInf;
-    if (intersectBisection(c, h.cur.t0, h.cur.t1, h.cur.nominalDeltaT, numValues, values, hit)) {
+    if (intersectBisection<LOOKAHEAD>(c, h.cur.t0, h.cur.t1, h.cur.nominalDeltaT, numValues, values, hit,
+                                      h.cacheT, h.cacheS)) {
       h.cur.t0         = hit.t + hit.epsilon;
       h.lastHitOffsetT = hit.t + hit.epsilon;
       return true;
     }
     h.cur.t0 = kPosInf;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Batched hit iteration as a per-lane state machine.  hitNextWith runs each
+// ray's loop nest (DDA, march, NaN nudges, bisection) to completion, so the
+// 32 random rays of a warp are soon in different loops and fewer than two
+// lanes execute each instruction.  Here every iteration of the warp's loop
+// first advances each lane through its non-sampling steps until the lane
+// needs one sample (or is done), then all lanes that need one take it at a
+// single call site.  Each lane performs exactly the steps, samples and
+// comparisons of hitNextWith in the same order, so hits are identical.
+// ---------------------------------------------------------------------------
+enum HitPhase : int {
+  kHpTop,          // a vklIterateHit call begins
+  kHpLoop,         // hitNext's interval loop
+  kHpStartSample,  // sample at the interval start arrived
+  kHpStartNudge,   // NaN start sample: nudge forward
+  kHpMarch,        // next march step
+  kHpMarchSample,  // march sample arrived
+  kHpMarchNudge,   // NaN march sample: nudge backward
+  kHpNudgeSample,  // nudged march sample arrived
+  kHpValue,        // test value i
+  kHpBisect,       // next bisection step
+  kHpBisectSample, // bisection sample arrived
+  kHpValueTail,    // end-point test of value i
+  kHpDone
+};
+
+template <class Hook>
+__device__ inline void hitsAllLanes(const DevGrid &g, const Hook &hook, uint32_t attr, const DevValueRanges &vr,
+                                    uint32_t numValues, const float *values, HitIt &h, bool active,
+                                    uint32_t maxPerRay, DevHit *out, uint32_t &count)
+{
+  const HitCtx<Hook> c{hook, h.o, h.d};
+  const float dlen = sqrtf(h.d.x * h.d.x + h.d.y * h.d.y + h.d.z * h.d.z);
+  int ph    = active ? kHpTop : kHpDone;
+  count     = 0;
+  // intersectBisection state
+  float t0 = 0.f, s0 = 0.f, tHi = 0.f, step = 0.f, hs = 0.f, t = 0.f, s = 0.f, ts = 0.f;
+  uint32_t march = 0;
+  int nudge      = 0;
+  uint32_t vi    = 0;
+  float tHit = kPosInf, eps = kPosInf, value = kPosInf, iso = 0.f;
+  // bisect state
+  float bt0 = 0.f, bs0 = 0.f, bt = 0.f, bs = 0.f, tol = 0.f, tMid = 0.f, tIso = kPosInf;
+  int iter     = 0;
+  float sample = 0.f, tReq = 0.f;
+  for (;;) {
+    bool want = false;
+    while (!want && ph != kHpDone) {
+      switch (ph) {
+      case kHpTop:
+        if (count >= kMaxHitsPerRay || numValues == 0 || h.cur.t0 == kPosInf) {
+          ph = kHpDone;
+          break;
+        }
+        ph = kHpLoop;
+        break;
+      case kHpLoop: {
+        const bool need = h.cur.t1 <= h.cur.t0;
+        bool have       = !need;
+        if (need)
+          have = intervalNext(g, attr, vr, h.ii, h.cur);
+        if (need && have) {
+          h.cur.t0 = maxx(h.cur.t0, h.lastHitOffsetT);
+          if (h.cur.t1 <= h.cur.t0)
+            break;  // next interval
+        }
+        if (!have) {
+          h.cur.t0 = kPosInf;
+          ph       = kHpDone;
+          break;
+        }
+        t0    = h.cur.t0;
+        tHi   = h.cur.t1;
+        step  = h.cur.nominalDeltaT;
+        nudge = 0;
+        march = 0;
+        if (t0 == h.cacheT) {
+          s0 = h.cacheS;
+          ph = kHpStartNudge;
+        } else {
+          tReq = t0;
+          want = true;
+          ph   = kHpStartSample;
+        }
+        break;
+      }
+      case kHpStartSample:
+        s0 = sample;
+        ph = kHpStartNudge;
+        break;
+      case kHpStartNudge:
+        if ((float)nudge < 10.f && isnan(s0) && t0 < tHi) {
+          t0 += maxx(1e-5f, 1e-5f * step);
+          ++nudge;
+          tReq = t0;
+          want = true;
+          ph   = kHpStartSample;
+        } else {
+          ph = kHpMarch;
+        }
+        break;
+      case kHpMarch:
+        if (!(t0 < tHi && march < kMaxMarchSteps)) {
+          h.cur.t0 = kPosInf;  // interval exhausted without a hit
+          ph       = kHpLoop;
+          break;
+        }
+        hs   = minx(step, tHi - t0);
+        t    = t0 + hs;
+        tReq = t;
+        want = true;
+        ph   = kHpMarchSample;
+        break;
+      case kHpMarchSample:
+        s        = sample;
+        h.cacheT = t;
+        h.cacheS = s;
+        ts       = t;
+        nudge    = 0;
+        ph       = kHpMarchNudge;
+        break;
+      case kHpMarchNudge:
+        if ((float)nudge < 10.f && isnan(s) && ts > t0) {
+          ts -= maxx(1e-5f, 1e-5f * step);
+          ++nudge;
+          tReq = ts;
+          want = true;
+          ph   = kHpNudgeSample;
+        } else {
+          tHit  = kPosInf;
+          eps   = kPosInf;
+          value = kPosInf;
+          vi    = 0;
+          ph    = kHpValue;
+        }
+        break;
+      case kHpNudgeSample:
+        s  = sample;
+        ph = kHpMarchNudge;
+        break;
+      case kHpValue:
+        if (vi == numValues) {
+          if (tHit < kPosInf) {
+            DevHit hit{tHit, value, eps * dlen};
+            if (count < maxPerRay)
+              out[count] = hit;
+            ++count;
+            h.cur.t0         = hit.t + hit.epsilon;
+            h.lastHitOffsetT = hit.t + hit.epsilon;
+            ph               = kHpTop;
+          } else {
+            t0 = t;
+            s0 = s;
+            ++march;
+            ph = kHpMarch;
+          }
+          break;
+        }
+        iso = __ldg(values + vi);
+        if (fabsf(s0 - iso) < 1e-6f) {
+          if (t0 < tHit && t0 <= tHi) {
+            tHit  = t0;
+            value = iso;
+            eps   = 0.125f * step;
+          }
+          ph = kHpValueTail;
+        } else if (!isnan(s0 + s) && (iso - s0) * (iso - s) < 0.f) {
+          bt0  = t0;
+          bs0  = s0;
+          bt   = ts;
+          bs   = s;
+          tol  = minx(1e-6f, 0.01f * hs);
+          iter = 0;
+          tMid = 0.f;
+          ph   = kHpBisect;
+        } else {
+          ph = kHpValueTail;
+        }
+        break;
+      case kHpBisect:
+        if (iter < 10) {
+          tMid              = 0.5f * (bt0 + bt);
+          const float error = 0.5f * (bt - bt0);
+          if (!(error < tol)) {
+            tReq = tMid;
+            want = true;
+            ph   = kHpBisectSample;
+            break;
+          }
+        }
+        tIso = tMid;
+        if (tIso < tHit && tIso <= tHi) {
+          tHit  = tIso;
+          value = iso;
+          eps   = 0.125f * step;
+        }
+        ph = kHpValueTail;
+        break;
+      case kHpBisectSample: {
+        const float sm = sample;
+        bool finished  = false;
+        if (isnan(sm)) {
+          tIso     = fabsf(iso - bs0) < fabsf(iso - bs) ? bt0 : bt;
+          finished = true;
+        } else if (sm == iso || (iso - bs0) * (iso - sm) < 0.f) {
+          bt = tMid;
+          bs = sm;
+        } else if (bs == iso || (iso - bs) * (iso - sm) < 0.f) {
+          bt0 = tMid;
+          bs0 = sm;
+        } else {
+          tIso     = kPosInf;
+          finished = true;
+        }
+        if (finished) {
+          if (tIso < tHit && tIso <= tHi) {
+            tHit  = tIso;
+            value = iso;
+            eps   = 0.125f * step;
+          }
+          ph = kHpValueTail;
+        } else {
+          ++iter;
+          ph = kHpBisect;
+        }
+        break;
+      }
+      case kHpValueTail:
+        if (t == tHi && fabsf(s - iso) < 1e-6f) {
+          if (ts < tHit && ts <= tHi) {
+            tHit  = ts;
+            value = iso;
+            eps   = 0.125f * step;
+          }
+        }
+        ++vi;
+        ph = kHpValue;
+        break;
+      default:
+        ph = kHpDone;
+        break;
+      }
+    }
+    if (!__any_sync(0xffffffffu, want))
+      return;
+    if (want)
+      sample = c.sampleAt(tReq);
+  }
+}
+
+__device__ inline bool hitNext(const DevGrid &g, int filter, uint32_t attr, uint32_t sampleDepth,
+                               const DevValueRanges &vr, uint32_t numValues, const float *values,
+                               HitIt &h, DevHit &hit)
+{
+  return hitNextWith<1>(g, AnySampleHook{&g, filter, attr, sampleDepth}, attr, vr, numValues, values, h, hit);
 }
 
 }  // namespace vklcuda

@@ -42,6 +42,14 @@ __global__ void __launch_bounds__(kBlock) kIntervals(const __grid_constant__ Dev
   counts[r] = c;
 }
 
+// Field specialisations of the batched hit kernel: the generic one samples
+// through the out-of-line type / filter dispatch; the float trilinear ones
+// inline their field (far fewer registers, so more rays in flight per SM)
+// and look LOOKAHEAD march steps ahead.  All give the same hits.
+enum HitKind { kHitAny = 0, kHitDenseFloatLinear = 1, kHitSparseFloatLinear = 2 };
+constexpr int kHitLookahead = 1;
+
+template <int KIND, int LOOKAHEAD>
 __global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid g, uint32_t attr,
                                                 int filter, uint32_t depth, DevValueRanges vr,
                                                 uint32_t numValues,
@@ -53,18 +61,36 @@ __global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid 
                                                 uint32_t *__restrict__ counts)
 {
   const uint64_t r = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-  if (r >= n)
-    return;
-  HitIt h;
-  hitInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), h);
-  uint32_t c = 0;
-  DevHit hit;
-  while (c < kMaxHitsPerRay && hitNext(g, filter, attr, kNumLevels - 1, vr, numValues, values, h, hit)) {
-    if (c < maxPerRay)
-      out[r * maxPerRay + c] = hit;
-    ++c;
+  if constexpr (KIND == kHitAny) {
+    if (r >= n)
+      return;
+    HitIt h;
+    hitInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), h);
+    uint32_t c = 0;
+    DevHit hit;
+    const AnySampleHook hook{&g, filter, attr, kNumLevels - 1};
+    while (c < kMaxHitsPerRay && hitNextWith<LOOKAHEAD>(g, hook, attr, vr, numValues, values, h, hit)) {
+      if (c < maxPerRay)
+        out[r * maxPerRay + c] = hit;
+      ++c;
+    }
+    counts[r] = c;
+  } else {
+    // every lane of the warp stays in the state machine's warp-wide loop
+    const bool active = r < n;
+    const uint64_t rr = active ? r : n - 1;
+    HitIt h;
+    hitInit(g, depth, ld3(orgs, rr), ld3(dirs, rr), __ldg(tr + 2 * rr), __ldg(tr + 2 * rr + 1), h);
+    uint32_t c = 0;
+    if constexpr (KIND == kHitDenseFloatLinear)
+      hitsAllLanes(g, LinearSampleHook<DenseField<float>>{&g, DenseField<float>(g, attr)}, attr, vr, numValues,
+                   values, h, active, maxPerRay, out + rr * maxPerRay, c);
+    else
+      hitsAllLanes(g, LinearSampleHook<SparseField<float>>{&g, SparseField<float>(g, attr, kNumLevels - 1)}, attr,
+                   vr, numValues, values, h, active, maxPerRay, out + rr * maxPerRay, c);
+    if (active)
+      counts[r] = c;
   }
-  counts[r] = c;
 }
 
 struct IntervalIterStateImpl {
@@ -134,8 +160,14 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
 {
   if (!n)
     return;
-  kHits<<<blocksFor(n), kBlock, 0, st>>>(g, attr, filter, depth, vr, numValues, values, n, origins,
-                                          directions, tRanges, maxPerRay, out, counts);
+  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && g.compress == kCompressNone;
+  auto k         = kHits<kHitAny, 1>;
+  if (lin && g.dense)
+    k = kHits<kHitDenseFloatLinear, kHitLookahead>;
+  else if (lin)
+    k = kHits<kHitSparseFloatLinear, kHitLookahead>;
+  k<<<blocksFor(n), kBlock, 0, st>>>(g, attr, filter, depth, vr, numValues, values, n, origins, directions,
+                                     tRanges, maxPerRay, out, counts);
   cudaCheck(cudaGetLastError(), "hit kernel launch");
 }
 

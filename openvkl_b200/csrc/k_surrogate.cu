@@ -6,7 +6,8 @@
 // MLP without biases, FP16 weights and activations on the tensor cores
 // (mma.sync m16n8k16, FP32 accumulation).  It is trained on samples of the
 // plain sampler (the caller supplies points and the plain samples as
-// targets), with the loss sum (y - target)^2 / n and Adam.  The plain sampler
+// targets), with the loss sum (y - target)^2 / n over the points with a
+// finite target, and Adam.  The plain sampler
 // is also the judge: calibration evaluates both on caller-supplied points
 // and flags every 32^3-voxel region whose largest error exceeds a threshold
 // (or that no calibration point reached); sampling with fallback returns the
@@ -502,8 +503,11 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
       forwardChunk(S.W, &S.X[0][0], kIn + 8, m0, g, t, y0, y1, &S.HT[0][0][0], kLdT);
       if (t == 0) {
         const uint64_t r0 = base + m0 + g, r1 = r0 + 8;
-        const float d0 = r0 < n ? y0 - __ldg(targets + r0) : 0.f;
-        const float d1 = r1 < n ? y1 - __ldg(targets + r1) : 0.f;
+        // points whose target is not finite (outside the data, where a
+        // sampler with an undefined background returns NaN) are ignored
+        const float t0 = r0 < n ? __ldg(targets + r0) : 0.f, t1 = r1 < n ? __ldg(targets + r1) : 0.f;
+        const float d0 = (r0 < n && isfinite(t0)) ? y0 - t0 : 0.f;
+        const float d1 = (r1 < n && isfinite(t1)) ? y1 - t1 : 0.f;
         S.dy[m0 + g]     = 2.f * d0;
         S.dy[m0 + g + 8] = 2.f * d1;
         lossAcc += d0 * d0 + d1 * d1;

@@ -158,6 +158,23 @@ struct DeviceBuffer {
 // ---------------------------------------------------------------------------
 // Device.
 // ---------------------------------------------------------------------------
+// Device scratch of binned sampling (launchSampleBinned): detection
+// counters, the binned entries of one pass, bin histogram and cursors.
+struct BinScratch {
+  DeviceBuffer counts, entries, bins;
+};
+
+// Binned sampling of incoherent point sets (k_bin.cu).  `applies` is the
+// cheap host test (dense float volume larger than L2, large call);
+// launchSampleBinned then measures the points' coherence on the device (one
+// small kernel and a 16-byte read-back, so it synchronizes `stream`) and,
+// for incoherent points, bins and samples them and returns true; for
+// coherent points it returns false and launches nothing else.  Points and
+// output are device memory; results equal launchSample's / launchGradient's.
+bool binnedSamplingApplies(const DevGrid &g, int filter, uint64_t n, uint32_t attr);
+bool launchSampleBinned(const DevGrid &g, int filter, uint64_t n, const float *pts, uint32_t attr,
+                        float *out, bool grad, BinScratch &scratch, cudaStream_t stream);
+
 struct Device {
   int cudaDevice = 0;
   cudaStream_t stream = nullptr;
@@ -186,6 +203,13 @@ struct Device {
   cudaEvent_t inReady[kPipeSlots]{}, computed[kPipeSlots]{}, drained[kPipeSlots]{};
   void ensurePipeline();
   ~Device();
+
+  // Scratch of binned sampling; `binMutex` serialises its users.  Binning
+  // is on by default for the calls it applies to; device parameter
+  // "binnedSampling" 0 turns it off.
+  std::mutex binMutex;
+  BinScratch binScratch;
+  bool binning = true;
 
   void setError(VKLError code, const std::string &msg);
   void log(int level, const std::string &msg);

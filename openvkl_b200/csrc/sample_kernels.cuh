@@ -70,6 +70,32 @@ __device__ __forceinline__ uint32_t tileKey(f3 p)
   return ((bx * 73856093u) ^ (by * 19349663u) ^ (bz * 83492791u)) & (kSortBins - 1);
 }
 
+// Exclusive scan of a tile's kSortBins-bin histogram in place (all
+// kTileThreads threads; 4 bins per thread, warp scans, then the warp totals).
+__device__ __forceinline__ void tileScan(int *hist)
+{
+  static_assert(kSortBins == 4 * kTileThreads && kSortBins == 1024, "scan layout");
+  __shared__ int warpSum[kTileThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int4 h   = reinterpret_cast<const int4 *>(hist)[threadIdx.x];
+  const int tot  = h.x + h.y + h.z + h.w;
+  int incl       = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o)
+      incl += t;
+  }
+  if (lane == 31)
+    warpSum[warp] = incl;
+  __syncthreads();
+  int before = incl - tot;
+  for (int w = 0; w < warp; ++w)
+    before += warpSum[w];
+  reinterpret_cast<int4 *>(hist)[threadIdx.x] =
+      make_int4(before, before + h.x, before + h.x + h.y, before + h.x + h.y + h.z);
+}
+
 template <typename T, bool DENSE, int FILTER, bool GRAD, int TILE>
 __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constant__ DevGrid g,
                                                             uint32_t maxDepth, uint64_t n,
@@ -119,30 +145,7 @@ __global__ void __launch_bounds__(kTileThreads) kSampleTile(const __grid_constan
   // after this barrier no thread reads the raw points again, so the scatter
   // may overwrite them
   __syncthreads();
-  {
-    // exclusive scan of the histogram: 4 bins per thread, warp scans, then
-    // the warp totals
-    static_assert(kSortBins == 4 * kTileThreads && kSortBins == 1024, "scan layout");
-    __shared__ int warpSum[kTileThreads / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int4 h   = reinterpret_cast<const int4 *>(hist)[threadIdx.x];
-    const int tot  = h.x + h.y + h.z + h.w;
-    int incl       = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o)
-        incl += t;
-    }
-    if (lane == 31)
-      warpSum[warp] = incl;
-    __syncthreads();
-    int before = incl - tot;
-    for (int w = 0; w < warp; ++w)
-      before += warpSum[w];
-    reinterpret_cast<int4 *>(hist)[threadIdx.x] =
-        make_int4(before, before + h.x, before + h.x + h.y, before + h.x + h.y + h.z);
-  }
+  tileScan(hist);
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < PPT; ++j) {

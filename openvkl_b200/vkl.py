@@ -269,6 +269,9 @@ class Device:
         return (self.lib.vklDeviceGetLastErrorCode(self.handle),
                 self.lib.vklDeviceGetLastErrorMsg(self.handle).decode())
 
+    def set_int(self, name: str, value: int):
+        self.lib.vklDeviceSetInt(self.handle, name.encode(), int(value))
+
     def set_stream(self, stream_ptr: int):
         self.lib.vklDeviceSetVoidPtr(self.handle, b"cudaStream", C.c_void_p(stream_ptr))
 

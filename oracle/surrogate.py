@@ -100,14 +100,17 @@ def forward(cfg, params, pts, fp16=False):
 
 
 def backward(cfg, params, pts, targets, fp16=False):
-    """Gradients of sum((y - t)^2): (loss, dtable (levels,T,2), dW1, dW2, dW3, dW4)."""
+    """Gradients of sum((y - t)^2) over the points with a finite target
+    (the others contribute nothing): (loss, dtable (levels,T,2), dW1, dW2,
+    dW3, dW4)."""
     table, W1, W2, W3, W4 = params
     W = [_h(np.asarray(w, np.float64), fp16) for w in (W1, W2, W3)]
     w4 = _h(np.asarray(W4, np.float64), fp16)
     y, acts = forward(cfg, params, pts, fp16)
     t = np.asarray(targets, np.float64)
-    loss = float(np.sum((y - t) ** 2))
-    dy = 2.0 * (y - t)
+    d = np.where(np.isfinite(t), y - np.where(np.isfinite(t), t, 0.0), 0.0)
+    loss = float(np.sum(d ** 2))
+    dy = 2.0 * d
     dW4 = acts[3].T @ dy
     g = _h(np.outer(dy, w4) * (acts[3] > 0), fp16)
     dW = [None, None, None]
