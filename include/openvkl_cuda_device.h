@@ -1,0 +1,149 @@
+// __device__ API of the cuda device: sampling and iteration called from an
+// application's own CUDA kernels, with the signatures of the reference's
+// GPU (SYCL) device API (openvkl/devices/gpu/include/openvkl/device/
+// openvkl.h:30-120).  The handles are passed by value into the kernel; their
+// `device` pointers address the objects' device-resident state, which
+// vklNew* / vklCommit write and which stays valid while the object lives.
+// After re-committing a volume, commit its samplers and contexts again.
+//
+// Two differences from the SYCL header, both forced by CUDA:
+// - Every function takes its VKLFeatureFlags argument explicitly. The host C
+//   API declares functions of the same names without it, and CUDA cannot
+//   overload on __host__ / __device__ alone.
+// - The iterator buffer sizes are the compile-time constants
+//   VKL_CUDA_INTERVAL_ITERATOR_SIZE / VKL_CUDA_HIT_ITERATOR_SIZE instead of
+//   vklGet*IteratorSize. The reference's GPU device publishes its
+//   VKL_MAX_*_ITERATOR_SIZE the same way (max_iterator_size.h).
+// Feature flags are accepted but not needed: the functions dispatch on the
+// volume's type at run time.  `time` is ignored (no temporal formats).
+//
+// Results are bit-identical to the host API's when the including
+// translation unit is compiled like the library: nvcc -gencode
+// arch=compute_100a,code=sm_100a --fmad=false -I<repo>/include.
+#pragma once
+#ifdef __CUDACC__
+
+#include "openvkl_cuda.h"
+#include "../openvkl_b200/csrc/iterate.cuh"
+
+#define VKL_CUDA_INTERVAL_ITERATOR_SIZE 512
+#define VKL_CUDA_HIT_ITERATOR_SIZE 768
+
+namespace vklcuda {
+namespace device_api {
+
+struct IntervalIteratorState {
+  IntervalIt it;
+  const DevIntervalContextState *ctx;
+};
+struct HitIteratorState {
+  HitIt h;
+  const DevHitContextState *ctx;
+};
+static_assert(sizeof(IntervalIteratorState) <= VKL_CUDA_INTERVAL_ITERATOR_SIZE, "interval iterator size");
+static_assert(sizeof(HitIteratorState) <= VKL_CUDA_HIT_ITERATOR_SIZE, "hit iterator size");
+
+__device__ __forceinline__ f3 toF3(const vkl_vec3f *v) { return {v->x, v->y, v->z}; }
+
+}  // namespace device_api
+}  // namespace vklcuda
+
+// Sample of one attribute at an object-space point (vklComputeSample).
+__device__ inline float vklComputeSample(const VKLSampler *sampler, const vkl_vec3f *objectCoordinates,
+                                         unsigned int attributeIndex, float time,
+                                         const VKLFeatureFlags featureFlags)
+{
+  (void)time;
+  (void)featureFlags;
+  const auto *st = (const vklcuda::DevSamplerState *)sampler->device;
+  return vklcuda::sampleObjectAny(st->g, st->s.filter, attributeIndex, st->s.maxSamplingDepth,
+                                  vklcuda::device_api::toF3(objectCoordinates));
+}
+
+// Samples of M attributes (vklComputeSampleM).
+__device__ inline void vklComputeSampleM(const VKLSampler *sampler, const vkl_vec3f *objectCoordinates,
+                                         float *samples, unsigned int M, const unsigned int *attributeIndices,
+                                         float time, const VKLFeatureFlags featureFlags)
+{
+  for (unsigned int m = 0; m < M; ++m)
+    samples[m] = vklComputeSample(sampler, objectCoordinates, attributeIndices[m], time, featureFlags);
+}
+
+// Object-space gradient with the sampler's gradient filter (vklComputeGradient).
+__device__ inline vkl_vec3f vklComputeGradient(const VKLSampler *sampler, const vkl_vec3f *objectCoordinates,
+                                               unsigned int attributeIndex, float time,
+                                               const VKLFeatureFlags featureFlags)
+{
+  (void)time;
+  (void)featureFlags;
+  const auto *st      = (const vklcuda::DevSamplerState *)sampler->device;
+  const vklcuda::f3 r = vklcuda::gradientObjectAny(st->g, st->s.gradientFilter, attributeIndex,
+                                                   st->s.maxSamplingDepth,
+                                                   vklcuda::device_api::toF3(objectCoordinates));
+  return vkl_vec3f{r.x, r.y, r.z};
+}
+
+// Interval iterator in a caller buffer of VKL_CUDA_INTERVAL_ITERATOR_SIZE
+// bytes (8-byte aligned), e.g. a local array.
+__device__ inline VKLIntervalIterator vklInitIntervalIterator(const VKLIntervalIteratorContext *context,
+                                                              const vkl_vec3f *origin,
+                                                              const vkl_vec3f *direction,
+                                                              const vkl_range1f *tRange, float time,
+                                                              void *buffer, const VKLFeatureFlags featureFlags)
+{
+  (void)time;
+  (void)featureFlags;
+  auto *s = (vklcuda::device_api::IntervalIteratorState *)buffer;
+  s->ctx  = (const vklcuda::DevIntervalContextState *)context->device;
+  vklcuda::intervalInit(s->ctx->sampler->g, s->ctx->depth, vklcuda::device_api::toF3(origin),
+                        vklcuda::device_api::toF3(direction), tRange->lower, tRange->upper, s->it);
+  return (VKLIntervalIterator)buffer;
+}
+
+__device__ inline int vklIterateInterval(VKLIntervalIterator iterator, VKLInterval *interval,
+                                         const VKLFeatureFlags featureFlags)
+{
+  (void)featureFlags;
+  auto *s = (vklcuda::device_api::IntervalIteratorState *)iterator;
+  vklcuda::DevInterval iv;
+  if (!vklcuda::intervalNext(s->ctx->sampler->g, s->ctx->attr, s->ctx->vr, s->it, iv))
+    return 0;
+  interval->tRange.lower     = iv.t0;
+  interval->tRange.upper     = iv.t1;
+  interval->valueRange.lower = iv.v0;
+  interval->valueRange.upper = iv.v1;
+  interval->nominalDeltaT    = iv.nominalDeltaT;
+  return 1;
+}
+
+// Hit iterator in a caller buffer of VKL_CUDA_HIT_ITERATOR_SIZE bytes.
+__device__ inline VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context, const vkl_vec3f *origin,
+                                                    const vkl_vec3f *direction, const vkl_range1f *tRange,
+                                                    float time, void *buffer, const VKLFeatureFlags featureFlags)
+{
+  (void)time;
+  (void)featureFlags;
+  auto *s = (vklcuda::device_api::HitIteratorState *)buffer;
+  s->ctx  = (const vklcuda::DevHitContextState *)context->device;
+  vklcuda::hitInit(s->ctx->sampler->g, s->ctx->depth, vklcuda::device_api::toF3(origin),
+                   vklcuda::device_api::toF3(direction), tRange->lower, tRange->upper, s->h);
+  return (VKLHitIterator)buffer;
+}
+
+__device__ inline int vklIterateHit(VKLHitIterator iterator, VKLHit *hit, const VKLFeatureFlags featureFlags)
+{
+  (void)featureFlags;
+  auto *s                   = (vklcuda::device_api::HitIteratorState *)iterator;
+  const auto *c             = s->ctx;
+  const vklcuda::DevGrid &g = c->sampler->g;
+  vklcuda::DevHit h;
+  if (!vklcuda::hitNext(g, c->sampler->s.filter, c->attr, vklcuda::kNumLevels - 1, c->vr, c->numValues,
+                        c->values, s->h, h))
+    return 0;
+  hit->t       = h.t;
+  hit->sample  = h.sample;
+  hit->epsilon = h.epsilon;
+  return 1;
+}
+
+#endif  // __CUDACC__

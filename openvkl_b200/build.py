@@ -32,9 +32,16 @@ SOURCES = ["api.cpp", "objects.cpp", "k_sample.cu", "k_sample_nearest.cu", "k_sa
            "k_bin.cu"]
 
 
+# The example renderers (a consumer of the __device__ API, built separately
+# from the device library they call into).
+RENDERERS = os.path.join(HERE, "renderers", "renderers.cu")
+RENDERERS_LIB = os.path.join(HERE, "libopenvkl_renderers.so")
+
+
 def _headers():
+    inc = os.path.join(HERE, "..", "include")
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] + [
-        os.path.join(HERE, "..", "include", "openvkl_cuda.h")]
+        os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
 
 
 def _stale(target, deps):
@@ -70,6 +77,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if force or _stale(RENDERERS_LIB, [RENDERERS] + _headers()):
+        cmd = [NVCC] + ARCH + FLAGS + ["-shared", "-o", RENDERERS_LIB, RENDERERS, "-lcudart_static", "-lrt",
+                                       "-lpthread", "-ldl"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for renderers.cu:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -719,7 +719,7 @@ VKLIntervalIteratorContext vklNewIntervalIteratorContext(VKLSampler sampler)
         c->device          = s->device;
         c->sampler         = Ref<Sampler>(s);
         c->commit();
-        return handleOf(c);
+        return handleOf(c, c->devState.ptr);
       },
       VKLIntervalIteratorContext{nullptr, nullptr});
 }
@@ -734,7 +734,7 @@ VKLHitIteratorContext vklNewHitIteratorContext(VKLSampler sampler)
         c->device     = s->device;
         c->sampler    = Ref<Sampler>(s);
         c->commit();
-        return handleOf(c);
+        return handleOf(c, c->devState.ptr);
       },
       VKLHitIteratorContext{nullptr, nullptr});
 }

@@ -155,6 +155,28 @@ struct DevValueRanges {
   const float *ranges;  // 2 floats per range (device)
 };
 
+// What a handle's `device` pointer addresses (device memory, written at the
+// object's commit, stable for the object's lifetime): the state the
+// __device__ API (include/openvkl_cuda_device.h) reads.
+struct DevSamplerState {
+  DevGrid g;
+  DevSampler s;
+};
+struct DevIntervalContextState {
+  const DevSamplerState *sampler;
+  DevValueRanges vr;
+  uint32_t attr;
+  uint32_t depth;
+};
+struct DevHitContextState {
+  const DevSamplerState *sampler;
+  DevValueRanges vr;
+  const float *values;
+  uint32_t numValues;
+  uint32_t attr;
+  uint32_t depth;
+};
+
 struct DevInterval {
   float t0, t1, v0, v1, nominalDeltaT;
 };

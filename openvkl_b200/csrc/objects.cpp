@@ -897,11 +897,10 @@ void Sampler::commit()
   for (int f : {s.filter, s.gradientFilter})
     if (f != kFilterNearest && f != kFilterLinear && f != kFilterCubic)
       fail("invalid filter");
-  struct {
-    DevGrid g;
-    DevSampler s;
-  } state{volume->grid, s};
-  devState.alloc(sizeof(state));
+  // the handle's device pointer stays valid across commits: allocate once
+  const DevSamplerState state{volume->grid, s};
+  if (!devState.ptr)
+    devState.alloc(sizeof(state));
   cudaCheck(cudaMemcpy(devState.ptr, &state, sizeof(state), cudaMemcpyHostToDevice), "upload");
 }
 
@@ -954,6 +953,11 @@ void IntervalContext::commit()
   if (!ranges.empty())
     cudaCheck(cudaMemcpy(devRanges.ptr, ranges.data(), ranges.size() * 4, cudaMemcpyHostToDevice),
               "upload");
+  const DevIntervalContextState state{sampler->devState.as<DevSamplerState>(), devValueRanges(), attr,
+                                      depth};
+  if (!devState.ptr)
+    devState.alloc(sizeof(state));
+  cudaCheck(cudaMemcpy(devState.ptr, &state, sizeof(state), cudaMemcpyHostToDevice), "upload");
 }
 
 DevValueRanges IntervalContext::devValueRanges() const
@@ -991,6 +995,11 @@ void HitContext::commit()
     cudaCheck(cudaMemcpy(devValues.ptr, values.data(), values.size() * 4, cudaMemcpyHostToDevice),
               "upload");
   }
+  const DevHitContextState state{sampler->devState.as<DevSamplerState>(), devValueRanges(),
+                                 devValues.as<float>(), (uint32_t)values.size(), attr, depth};
+  if (!devState.ptr)
+    devState.alloc(sizeof(state));
+  cudaCheck(cudaMemcpy(devState.ptr, &state, sizeof(state), cudaMemcpyHostToDevice), "upload");
 }
 
 DevValueRanges HitContext::devValueRanges() const

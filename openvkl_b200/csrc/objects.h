@@ -274,7 +274,7 @@ struct Volume : ManagedObject {
 struct Sampler : ManagedObject {
   Ref<Volume> volume;
   DevSampler s{};
-  DeviceBuffer devState;  // {DevGrid, DevSampler} for the device-side API
+  DeviceBuffer devState;  // DevSamplerState for the device-side API
   const char *typeName() const override { return "Sampler"; }
   void commit() override;
 };
@@ -287,6 +287,7 @@ struct IntervalContext : ManagedObject {
   uint32_t depth    = 2;
   bool elementary   = false;
   DeviceBuffer devRanges;
+  DeviceBuffer devState;  // DevIntervalContextState for the device-side API
   const char *typeName() const override { return "IntervalIteratorContext"; }
   void commit() override;
   DevValueRanges devValueRanges() const;
@@ -300,6 +301,7 @@ struct HitContext : ManagedObject {
   float minMax[2] = {0, 0};
   uint32_t depth  = 2;
   DeviceBuffer devRanges, devValues;
+  DeviceBuffer devState;  // DevHitContextState for the device-side API
   const char *typeName() const override { return "HitIteratorContext"; }
   void commit() override;
   DevValueRanges devValueRanges() const;

@@ -627,6 +627,53 @@ __device__ __forceinline__ float sampleIndexAny(const DevGrid &g, int filter, ui
   return sampleFiltered(SparseField<float>(g, attr, depth), filter, cc, p);
 }
 
+// Object-space gradient with runtime type dispatch: the index-space
+// gradient of the filter (zero for nearest) through xfmNormal, as the
+// gradient kernels compute it (VdbSampler.ispc:276-301).
+template <class Field>
+__device__ __forceinline__ f3 gradientFiltered(const DevGrid &g, const Field &F, int filter, f3 p)
+{
+  if (filter == kFilterNearest)
+    return {0.f, 0.f, 0.f};
+  const f3 gi = filter == kFilterCubic ? gradientCubic(F, p) : gradientLinear(F, p);
+  return xfmNormal(g.objectToIndex, gi);
+}
+
+__device__ __forceinline__ f3 gradientObjectAny(const DevGrid &g, int filter, uint32_t attr, uint32_t depth, f3 oc)
+{
+  const f3 p       = xfmPoint(g.objectToIndex, oc);
+  const uint32_t t = g.type[attr];
+  if (g.dense) {
+    switch (t) {
+    case kUChar:
+      return gradientFiltered(g, DenseField<uint8_t>(g, attr), filter, p);
+    case kShort:
+      return gradientFiltered(g, DenseField<int16_t>(g, attr), filter, p);
+    case kUShort:
+      return gradientFiltered(g, DenseField<uint16_t>(g, attr), filter, p);
+    case kHalf:
+      return gradientFiltered(g, DenseField<__half>(g, attr), filter, p);
+    case kDouble:
+      return gradientFiltered(g, DenseField<double>(g, attr), filter, p);
+    default:
+      return gradientFiltered(g, DenseField<float>(g, attr), filter, p);
+    }
+  }
+  switch (g.compress) {
+  case kCompressFP16:
+    return gradientFiltered(g, SparseField<CodeFP16>(g, attr, depth), filter, p);
+  case kCompressBF16:
+    return gradientFiltered(g, SparseField<CodeBF16>(g, attr, depth), filter, p);
+  case kCompressFP8:
+    return gradientFiltered(g, SparseField<CodeE4M3>(g, attr, depth), filter, p);
+  default:
+    break;
+  }
+  if (t == kHalf)
+    return gradientFiltered(g, SparseField<__half>(g, attr, depth), filter, p);
+  return gradientFiltered(g, SparseField<float>(g, attr, depth), filter, p);
+}
+
 __device__ __forceinline__ float sampleObjectAny(const DevGrid &g, int filter, uint32_t attr,
                                                  uint32_t depth, f3 oc)
 {

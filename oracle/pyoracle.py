@@ -84,6 +84,8 @@ def lib(fast: bool = False) -> C.CDLL:
         L.orc_sample_fp64.argtypes = [P, C.c_int, U64, P, U32, P]
         L.orc_iterate_intervals.argtypes = [P, U32, U32, P, F32, U64, P, P, P, U32, P, P]
         L.orc_iterate_hits.argtypes = [P, U32, C.c_int, U32, P, U64, P, P, P, U32, P, P]
+        L.orc_render.argtypes = [P, C.c_int, C.c_int, C.c_int, U32, U32, U32, P, F32, U32, P, P, P, C.c_int, P,
+                                 P, P, P]
         L.orc_tricubic_map.restype = C.c_int
         L.orc_tricubic_map.argtypes = [P, P, P]
         L.orc_inner_nodes.restype = U64
@@ -243,6 +245,24 @@ class OracleVolume:
         self._lib.orc_iterate_hits(self._h, attr, filter, len(v), _p(v), len(o), _p(o), _p(d),
                                    _p(t), max_hits, _p(out), _p(cnt))
         return out, cnt
+
+    def render(self, renderer, camera, tf_colors, tf_range, width, height, bounds, filter=FILTER_LINEAR,
+               gradient_filter=None, max_sampling_depth=3, attr=0, value_ranges=None, hint=0.5, iso_values=(),
+               sampling_rate=1.0, interval_color_scale=4.0, interval_opacity=0.25, first_interval_only=False,
+               show_interval_borders=False):
+        """The example renderers restated (orc_render): (height, width, 4) RGBA float32."""
+        vr = None if value_ranges is None else np.ascontiguousarray(value_ranges, np.float32).reshape(-1, 2)
+        iso = np.ascontiguousarray(iso_values, np.float32).reshape(-1)
+        cam = np.ascontiguousarray(camera, np.float32).reshape(14)
+        tfc = np.ascontiguousarray(tf_colors, np.float32).reshape(-1, 4)
+        tfr = np.ascontiguousarray(tf_range, np.float32).reshape(2)
+        ip = np.array([width, height, int(first_interval_only), int(show_interval_borders)], np.int32)
+        fp = np.array(list(bounds) + [sampling_rate, interval_color_scale, interval_opacity], np.float32)
+        out = np.zeros((height, width, 4), np.float32)
+        self._lib.orc_render(self._h, renderer, filter, filter if gradient_filter is None else gradient_filter,
+                             max_sampling_depth, attr, 0 if vr is None else len(vr), _p(vr), hint, len(iso),
+                             _p(iso), _p(cam), _p(tfc), len(tfc), _p(tfr), _p(ip), _p(fp), _p(out))
+        return out
 
     def inner_nodes(self, max_depth=1, attr=0):
         n = int(self._lib.orc_inner_nodes(self._h, max_depth, attr, 0, None))

@@ -1674,76 +1674,290 @@ void orc_iterate_intervals(const OrcVolume *v, uint32_t attr, uint32_t numRanges
   });
 }
 
+namespace {
+
+// Default hit iterator state and one vklIterateHit call
+// (DefaultIterator.ispc:140-258).
+struct HitIter {
+  IntervalIt it;
+  Interval cur;
+  float lastHitOffsetT;
+  vec3f o, d;
+};
+
+ValueRanges hitRanges(const float *values, uint32_t numValues)
+{
+  // HitIteratorContext::commit (IteratorContext.cpp:266-336): degenerate
+  // ranges at the iso values
+  ValueRanges vr;
+  for (uint32_t i = 0; i < numValues; ++i)
+    vr.ranges.push_back({values[i], values[i]});
+  vr.computeMinMax();
+  return vr;
+}
+
+int hitDepth(const Grid &g) { return g.dense ? hintToDepth(0.5f) : hintToDepth(1.f); }
+
+void hitInit(HitIter &h, const Grid &g, uint32_t attr, const vec3f &o, const vec3f &d, const range1f &tr)
+{
+  intervalInit(h.it, g, attr, (uint32_t)hitDepth(g), o, d, tr);
+  h.cur.t             = {1.f, -1.f};
+  h.cur.v             = {0.f, 0.f};
+  h.cur.nominalDeltaT = 0.f;
+  h.lastHitOffsetT    = -std::numeric_limits<float>::infinity();
+  h.o                 = o;
+  h.d                 = d;
+}
+
+bool hitNext(HitIter &h, const Grid &g, int filter, uint32_t attr, const ValueRanges &vr,
+             const std::vector<float> &vals, HitRec &out)
+{
+  const float inf = std::numeric_limits<float>::infinity();
+  if (vals.empty() || h.cur.t.lower == inf)
+    return false;
+  for (;;) {
+    const bool need = h.cur.t.upper <= h.cur.t.lower;
+    bool have       = !need;
+    if (need)
+      have = intervalIterate(h.it, vr, h.cur);
+    if (need && have) {
+      h.cur.t.lower = fmax_(h.cur.t.lower, h.lastHitOffsetT);
+      if (h.cur.t.upper <= h.cur.t.lower)
+        continue;
+    }
+    if (!have) {
+      h.cur.t.lower = inf;
+      return false;
+    }
+    HitRec hit{inf, 0.f, 0.f};
+    if (intersectBisection(g, filter, attr, h.o, h.d, h.cur.t, h.cur.nominalDeltaT, vals, hit)) {
+      h.cur.t.lower    = hit.t + hit.epsilon;
+      h.lastHitOffsetT = hit.t + hit.epsilon;
+      out              = hit;
+      return true;
+    }
+    h.cur.t.lower = inf;
+  }
+}
+
+}  // namespace
+
 void orc_iterate_hits(const OrcVolume *v, uint32_t attr, int filter, uint32_t numValues,
                       const float *values, uint64_t numRays, const float *origins,
                       const float *directions, const float *tRanges, uint32_t maxHits,
                       float *out, uint32_t *counts)
 {
   const Grid &g = v->g;
-  // HitIteratorContext::commit (IteratorContext.cpp:266-336): degenerate
-  // ranges, depth 2 (hint 0.5) for dense, 3 (hint 1.0) for sparse VDB.
-  ValueRanges vr;
-  std::vector<float> vals(values, values + numValues);
-  for (uint32_t i = 0; i < numValues; ++i)
-    vr.ranges.push_back({values[i], values[i]});
-  vr.computeMinMax();
-  const int depth = g.dense ? hintToDepth(0.5f) : hintToDepth(1.f);
-  const float inf = std::numeric_limits<float>::infinity();
+  const ValueRanges vr = hitRanges(values, numValues);
+  const std::vector<float> vals(values, values + numValues);
   parallelFor((int64_t)numRays, 0, 64, [&](int64_t r) {
-    const vec3f o = {origins[3 * r], origins[3 * r + 1], origins[3 * r + 2]};
-    const vec3f d = {directions[3 * r], directions[3 * r + 1], directions[3 * r + 2]};
-    IntervalIt it;
-    intervalInit(it, g, attr, (uint32_t)depth, o, d, {tRanges[2 * r], tRanges[2 * r + 1]});
-    Interval cur;
-    cur.t     = {1.f, -1.f};
-    cur.v     = {0.f, 0.f};
-    cur.nominalDeltaT = 0.f;
-    float lastHitOffsetT = -inf;
-    uint32_t c           = 0;
-    if (numValues == 0) {
-      counts[r] = 0;
-      return;
-    }
-    while (c < MAX_HITS) {
-      // one vklIterateHit call
-      if (cur.t.lower == inf)
-        break;
-      bool found = false, done = false;
-      for (;;) {
-        const bool need = cur.t.upper <= cur.t.lower;
-        bool have       = !need;
-        if (need)
-          have = intervalIterate(it, vr, cur);
-        if (need && have) {
-          cur.t.lower = fmax_(cur.t.lower, lastHitOffsetT);
-          if (cur.t.upper <= cur.t.lower)
-            continue;
-        }
-        if (!have) {
-          cur.t.lower = inf;
-          done        = true;
-          break;
-        }
-        HitRec hit{inf, 0.f, 0.f};
-        if (intersectBisection(g, filter, attr, o, d, cur.t, cur.nominalDeltaT, vals, hit)) {
-          cur.t.lower    = hit.t + hit.epsilon;
-          lastHitOffsetT = hit.t + hit.epsilon;
-          if (c < maxHits) {
-            float *h = out + ((uint64_t)r * maxHits + c) * 3;
-            h[0] = hit.t;
-            h[1] = hit.sample;
-            h[2] = hit.epsilon;
-          }
-          c++;
-          found = true;
-          break;
-        }
-        cur.t.lower = inf;
+    HitIter h;
+    hitInit(h, g, attr, {origins[3 * r], origins[3 * r + 1], origins[3 * r + 2]},
+            {directions[3 * r], directions[3 * r + 1], directions[3 * r + 2]},
+            {tRanges[2 * r], tRanges[2 * r + 1]});
+    uint32_t c = 0;
+    HitRec hit;
+    while (c < MAX_HITS && hitNext(h, g, filter, attr, vr, vals, hit)) {
+      if (c < maxHits) {
+        float *o = out + ((uint64_t)r * maxHits + c) * 3;
+        o[0]     = hit.t;
+        o[1]     = hit.sample;
+        o[2]     = hit.epsilon;
       }
-      if (done || !found)
-        break;
+      c++;
     }
     counts[r] = c;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// The reference's example renderers, one ray per pixel centre
+// (examples/interactive/renderer: Camera.ih Camera_createRay;
+// RendererGpuKernel.h:64-93 sampleTransferFunction and :142-155
+// intersectBox; RayMarchIteratorGpuKernel.cpp:9-88;
+// IntervalIteratorDebugGpuKernel.cpp:9-77; HitIteratorRendererGpuKernel.cpp:
+// 9-114).  The reference's approximate reciprocals and rsqrt are exact
+// divisions and square roots here; min/max of possibly-NaN slab values use
+// the IEEE minNum / maxNum form (std::fmin / std::fmax).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RV3 {
+  float x, y, z;
+};
+inline RV3 operator+(RV3 a, RV3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline RV3 operator-(RV3 a, RV3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline RV3 operator*(float s, RV3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline float rdot(RV3 a, RV3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline RV3 rnormalize(RV3 a)
+{
+  const float l = std::sqrt(rdot(a, a));
+  return {a.x / l, a.y / l, a.z / l};
+}
+inline float clamp01(float x) { return std::fmin(std::fmax(x, 0.f), 1.f); }
+
+struct RenderTF {
+  const float *c;
+  int n;
+  float lo, hi;
+  void at(float value, float out[4]) const
+  {
+    if (std::isnan(value) || n == 0) {
+      out[0] = out[1] = out[2] = out[3] = 0.f;
+      return;
+    }
+    const int last = n - 1;
+    if (value <= lo) {
+      std::memcpy(out, c, 16);
+      return;
+    }
+    if (value >= hi) {
+      std::memcpy(out, c + 4 * last, 16);
+      return;
+    }
+    value                 = (value - lo) / (hi - lo) * (float)last;
+    const int index       = (int)std::floor(value);
+    const float remainder = value - (float)index;
+    const int next        = std::min(index + 1, last);
+    const float a         = 1.f - remainder;
+    for (int k = 0; k < 4; ++k)
+      out[k] = a * c[4 * index + k] + remainder * c[4 * next + k];
+  }
+};
+
+}  // namespace
+
+void orc_render(const OrcVolume *v, int renderer, int filter, int gradientFilter, uint32_t maxSamplingDepth,
+                uint32_t attr, uint32_t numRanges, const float *ranges, float hint, uint32_t numValues,
+                const float *values, const float camera[14], const float *tfColors, int tfNum,
+                const float tfRange[2], const int ip[4], const float fp[9], float *rgba)
+{
+  const Grid &g = v->g;
+  const int W = ip[0], H = ip[1];
+  const bool firstOnly = ip[2] != 0, borders = ip[3] != 0;
+  const float *bounds = fp;
+  const float samplingRate = fp[6], colorScale = fp[7], intervalOpacity = fp[8];
+  const RenderTF tf{tfColors, tfNum, tfRange[0], tfRange[1]};
+  ValueRanges ivr;
+  for (uint32_t i = 0; i < numRanges; ++i)
+    ivr.ranges.push_back({ranges[2 * i], ranges[2 * i + 1]});
+  ivr.computeMinMax();
+  const ValueRanges hvr = hitRanges(values, numValues);
+  const std::vector<float> vals(values, values + numValues);
+  const int depth = hintToDepth(hint);
+  const float inf = std::numeric_limits<float>::infinity();
+  auto sampleP = [&](RV3 c) { return sampleAt(g, filter, xfmPoint(g.o2i, {c.x, c.y, c.z}), attr, maxSamplingDepth); };
+  auto gradientP = [&](RV3 c) {
+    if (gradientFilter == F_NEAREST)
+      return RV3{0.f, 0.f, 0.f};
+    const vec3f p  = xfmPoint(g.o2i, {c.x, c.y, c.z});
+    const vec3f gi = gradientFilter == F_CUBIC ? gradientCubic(g, p, attr, maxSamplingDepth)
+                                               : gradientLinear(g, p, attr, maxSamplingDepth);
+    const vec3f r = xfmNormal(g.o2i, gi);
+    return RV3{r.x, r.y, r.z};
+  };
+  parallelFor((int64_t)W * H, 0, 16, [&](int64_t idx) {
+    // Camera_createRay at the pixel centre
+    const float px = (float)(idx % W) + 0.5f, py = (float)(idx / W) + 0.5f;
+    const float irx    = 1.f / (float)W;
+    const float sx     = (px - 0.5f * (float)W) * irx;
+    const float sy     = -(py - 0.5f * (float)H) * irx;
+    const RV3 pCamera  = {camera[0] * sx, camera[0] * sy, 0.f};
+    const RV3 pAperture = {0.f, 0.f, -camera[1]};
+    const RV3 dCamera  = pAperture - pCamera;
+    const RV3 R0 = {camera[2], camera[3], camera[4]}, R1 = {camera[5], camera[6], camera[7]},
+              R2 = {camera[8], camera[9], camera[10]};
+    const RV3 org = {rdot(R0, pCamera) + camera[11], rdot(R1, pCamera) + camera[12],
+                     rdot(R2, pCamera) + camera[13]};
+    const RV3 dir = rnormalize({rdot(R0, dCamera), rdot(R1, dCamera), rdot(R2, dCamera)});
+    // intersectBox
+    const float rx = 1.f / dir.x, ry = 1.f / dir.y, rz = 1.f / dir.z;
+    const float x0 = (bounds[0] - org.x) * rx, y0 = (bounds[1] - org.y) * ry, z0 = (bounds[2] - org.z) * rz;
+    const float x1 = (bounds[3] - org.x) * rx, y1 = (bounds[4] - org.y) * ry, z1 = (bounds[5] - org.z) * rz;
+    range1f tr;
+    tr.lower = std::fmax(std::fmax(std::fmax(std::fmin(x0, x1), std::fmin(y0, y1)), std::fmin(z0, z1)), 0.f);
+    tr.upper = std::fmin(std::fmin(std::fmin(std::fmax(x0, x1), std::fmax(y0, y1)), std::fmax(z0, z1)), inf);
+    RV3 color   = {0.f, 0.f, 0.f};
+    float alpha = 0.f;
+    if (renderer == 0 || renderer == 1) {
+      IntervalIt it;
+      intervalInit(it, g, attr, (uint32_t)depth, {org.x, org.y, org.z}, {dir.x, dir.y, dir.z}, tr);
+      Interval iv;
+      int count = 0;
+      while (intervalIterate(it, ivr, iv) && alpha < 0.99f) {
+        if (renderer == 0) {
+          const float dtn = iv.nominalDeltaT / samplingRate;
+          float lo = iv.t.lower, hi = std::fmin(iv.t.lower + dtn, iv.t.upper);
+          while (hi - lo > 0.f && alpha < 0.99f) {
+            const float t  = 0.5f * (lo + hi);
+            const float dt = hi - lo;
+            float sc[4];
+            tf.at(sampleP(org + t * dir), sc);
+            const float op = clamp01(sc[3] * dt);
+            color          = color + (1.f - alpha) * RV3{sc[0] * op, sc[1] * op, sc[2] * op};
+            alpha          = alpha + (1.f - alpha) * op;
+            lo             = hi;
+            hi             = std::fmin(lo + dtn, iv.t.upper);
+          }
+        } else {
+          count++;
+          const float dt = iv.t.upper - iv.t.lower;
+          float sc[4];
+          tf.at(tfRange[0] + (float)count / colorScale * (tfRange[1] - tfRange[0]), sc);
+          sc[3]    = intervalOpacity;
+          float op = clamp01(sc[3] * dt);
+          RV3 c    = {sc[0] * op, sc[1] * op, sc[2] * op};
+          if (borders && dt < iv.nominalDeltaT) {
+            c  = {1.f, 1.f, 1.f};
+            op = 1.f;
+          }
+          color = color + (1.f - alpha) * c;
+          alpha = alpha + (1.f - alpha) * op;
+          if (firstOnly)
+            break;
+        }
+      }
+    } else {
+      const float surfaceAlpha = 0.6f;
+      const float emission[2]  = {1.f, 0.8f};
+      const RV3 lightDir[2]    = {rnormalize({1.f, 1.f, 1.f}), rnormalize({1.f, 1.f, -1.f})};
+      HitIter h;
+      hitInit(h, g, attr, {org.x, org.y, org.z}, {dir.x, dir.y, dir.z}, tr);
+      HitRec hit;
+      while (hitNext(h, g, filter, attr, hvr, vals, hit) && alpha < 0.99f) {
+        const RV3 c = org + hit.t * dir;
+        RV3 N       = rnormalize(gradientP(c));
+        if (std::isnan(N.x) || std::isnan(N.y) || std::isnan(N.z))
+          N = {0.f, 0.f, 0.f};
+        const RV3 wi   = rnormalize({-1.f * dir.x, -1.f * dir.y, -1.f * dir.z});
+        const float ci = rdot(N, wi);
+        float illum    = 0.f;
+        if (std::sqrt(rdot(N, N)) > 0.f) {
+          illum = 0.1f;
+          for (int i = 0; i < 2; ++i) {
+            const RV3 wo   = lightDir[i];
+            const float co = rdot(N, wo);
+            if ((co > 0.f) == (ci > 0.f)) {
+              HitIter sh;
+              hitInit(sh, g, attr, {c.x, c.y, c.z}, {wo.x, wo.y, wo.z}, {hit.epsilon, inf});
+              HitRec shadow;
+              if (!hitNext(sh, g, filter, attr, hvr, vals, shadow))
+                illum += std::fabs(co) * emission[i];
+            }
+          }
+        } else {
+          illum = 1.f;
+        }
+        float sc[4];
+        tf.at(hit.sample, sc);
+        color = color + ((1.f - alpha) * illum) * RV3{sc[0], sc[1], sc[2]};
+        alpha = alpha + (1.f - alpha) * surfaceAlpha;
+      }
+    }
+    rgba[4 * idx]     = color.x;
+    rgba[4 * idx + 1] = color.y;
+    rgba[4 * idx + 2] = color.z;
+    rgba[4 * idx + 3] = 1.f;
   });
 }
 

@@ -147,6 +147,19 @@ void orc_iterate_hits(const OrcVolume *v,
                       float *out,
                       uint32_t *counts);
 
+// The reference's example renderers restated (one ray per pixel centre):
+// renderer 0 ray march iterator, 1 interval iterator debug, 2 hit iterator
+// renderer.  camera = {sensorWidth, focalLength, camera-to-world rotation
+// rows (9), translation (3)}; tfColors = tfNum RGBA quadruples over
+// tfRange; ip = {width, height, firstIntervalOnly, showIntervalBorders};
+// fp = {bounds (6), samplingRate, intervalColorScale, intervalOpacity}.
+// Interval context: numRanges ranges and the resolution hint; hit context:
+// numValues iso values.  Writes width*height RGBA floats, row 0 at the top.
+void orc_render(const OrcVolume *v, int renderer, int filter, int gradientFilter, uint32_t maxSamplingDepth,
+                uint32_t attr, uint32_t numRanges, const float *ranges, float hint, uint32_t numValues,
+                const float *values, const float camera[14], const float *tfColors, int tfNum,
+                const float tfRange[2], const int ip[4], const float fp[9], float *rgba);
+
 // Tricubic coefficient map as generated here: for row r (coefficient
 // 16i+4j+k) entries [start[r], start[r+1]) of (col, weight).
 int orc_tricubic_map(int32_t *start, int32_t *cols, float *weights);

@@ -61,3 +61,32 @@ def test_no_device_without_gpu(lib_path):
     L = vkl.load_library(lib_path)
     assert not L.vklNewDevice(b"cuda")
     assert not L.vklNewDevice(b"cpu")
+
+
+def test_renderer_library_exports_and_device_header_compiles(lib_path):
+    """The example renderer library (a consumer of include/openvkl_cuda_device.h)
+    builds for sm_100a and exports its two entry points."""
+    from openvkl_b200 import build
+    assert os.path.exists(build.RENDERERS_LIB)
+    out = subprocess.run(["nm", "-D", "--defined-only", build.RENDERERS_LIB], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if l.strip()}
+    assert {"vklExampleRender", "vklExampleSamplePoints"} <= exported
+
+
+def test_oracle_renderer_draws_the_volume():
+    """The oracle's restated ray march renderer shades pixels that see the
+    volume and leaves the others black (no GPU needed)."""
+    import numpy as np
+    from oracle import pyoracle as O
+    from openvkl_b200 import render
+    from openvkl_b200.fields import sinusoid_field
+    vox = sinusoid_field((24, 20, 28), seed=3)
+    ref = O.OracleVolume.dense_volume(vox)
+    b = ref.info()["bounds"]
+    lo, hi = float(vox.min()), float(vox.max())
+    cam = render.orbit_camera(b, 40, 30, distance=3.0)
+    img = ref.render(0, cam.as_array(), render.DEFAULT_TF, (lo, hi), 40, 30, b, value_ranges=[[lo, hi]])
+    assert np.isfinite(img).all()
+    lit = img[:, :, :3].sum(-1) > 0
+    assert lit[15, 20] and not lit[0, 0]
