@@ -45,7 +45,8 @@ METRIC = "Gsamples/s and HBM GB/s (% roofline): plain FP32 vs FP16/FP8/batched/M
 UNIT = "Gsamples/s"
 MAX_CPU_POINTS = 1 << 27  # bounded CPU sample (1.6 GB of points)
 FILTER = {"coherent": 100, "incoherent": 100, "cubic": 200, "gradient": 100, "vdb": 100, "batched": 100,
-          "intervals": 100, "hits": 100, "surrogate": 100}
+          "intervals": 100, "hits": 100, "surrogate": 100,
+          "render": 100, "config1": 100}
 BATCH_VOLUMES = 512
 VDB_DOMAIN, VDB_POINTS = 4096, 1 << 26
 HIT_RAYS = 1 << 24
@@ -789,6 +790,98 @@ def run_surrogate(args):
     sur.release()
 
 
+def run_render(args):
+    """The reference's example renderers on the __device__ API, headless:
+    1920x1080 frames of the 1024^3 volume from the orbit camera, one ray per
+    pixel; ray march iterator (sampling rate 1, interval context over the
+    whole value range), interval iterator debug and hit iterator renderer
+    (isovalues at 40 % and 70 % of the value range).  value = ray-march
+    Mpixels/s; each renderer's frame time beside it."""
+    import torch
+    from openvkl_b200 import render, vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vox = volume_numpy()
+    vol = vkl.structured_regular(dev, torch.from_numpy(vox).cuda(), shared=True)
+    smp = vkl.Sampler(vol, filter=100, gradient_filter=100)
+    lo, hi = (float(x) for x in vol.value_range())
+    ictx = vkl.IntervalIteratorContext(smp, value_ranges=[[lo, hi]])
+    hctx = vkl.HitIteratorContext(smp, [lo + 0.4 * (hi - lo), lo + 0.7 * (hi - lo)])
+    cam = render.orbit_camera(vol.bounding_box(), WIDTH, HEIGHT)
+    tf = render.transfer_function((lo, hi))
+    out = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, device="cuda")
+    times = {}
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        for name in ("ray_march", "interval_debug", "hits"):
+            fn = lambda: render.render(name, smp, cam, WIDTH, HEIGHT, tf=tf, interval_context=ictx,
+                                       hit_context=hctx, out=out, stream=stream.cuda_stream)
+            times[name] = _timed_device(fn, args.steps, args.warmup, stream)
+    px = WIDTH * HEIGHT
+    line = {"metric": METRIC, "value": px / (times["ray_march"] * 1e-3) / 1e6, "unit": "Mpixels/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": times["ray_march"],
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded sinusoid volume)",
+            "config": {"workload": f"example renderers on the __device__ API, {WIDTH}x{HEIGHT}, structuredRegular "
+                                   f"{DIMS[0]}^3 float32, one ray per pixel"},
+            "frame_ms": times, "gpu_launches": 3 * args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_config1(args):
+    """128^3 float32 vertex-centered structuredRegular (the seeded sinusoid
+    field), 2^20 points uniform in the object bounds, trilinear
+    vklComputeSampleN + vklComputeGradientN per step (the configuration the
+    reference's CPU device runs).  value = points/s with both a sample and a
+    gradient; the oracle on all host threads beside it."""
+    import torch
+    from openvkl_b200 import fields, vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vox = volume_numpy((128, 128, 128))
+    vol = vkl.structured_regular(dev, torch.from_numpy(vox).cuda())
+    smp = vkl.Sampler(vol, filter=100, gradient_filter=100)
+    n = 1 << 20
+    pts_np = fields.uniform_points(n, (0, 0, 0), (127, 127, 127), seed=2)
+    pts = torch.from_numpy(pts_np).cuda()
+    s = torch.empty(n, device="cuda")
+    g = torch.empty((n, 3), device="cuda")
+
+    def step():
+        smp.sample(pts, out=s)
+        smp.gradient(pts, out=g)
+
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        ms = _timed_device(step, max(args.steps, 100), args.warmup, stream)
+    base = None
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        ref = O.OracleVolume.dense_volume(vox, fast=True)
+        L = O.lib(True)
+        threads = os.cpu_count() or 1
+        out_s = np.empty(n, np.float32)
+        out_g = np.empty((n, 3), np.float32)
+        t0 = time.perf_counter()
+        L.orc_sample_parallel(ref._h, 100, n, pts_np.ctypes.data, 0, out_s.ctypes.data, threads)
+        _threaded_oracle(lambda a, b: L.orc_gradient(ref._h, 100, 3, b - a, pts_np[a:b].ctypes.data, 0,
+                                                     out_g[a:b].ctypes.data), n, threads, chunk=1 << 14)
+        dt = time.perf_counter() - t0
+        base = {"value": n / dt / 1e9, "unit": "Gpoints/s (sample + gradient)", "cores": threads, "kind": "port",
+                "sample": f"all {n} points; oracle C++ restatement of the reference CPU device, -O3 "
+                          f"-march=native, {threads} host threads, {dt:.2f} s"}
+    line = {"metric": METRIC, "value": n / (ms * 1e-3) / 1e9, "unit": "Gpoints/s (sample + gradient)",
+            "n_gpus": 1, "steps": max(args.steps, 100), "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded sinusoid volume, uniform points)",
+            "config": {"workload": "structuredRegular 128^3 float32 vertex-centered, 2^20 uniform points, "
+                                   "trilinear sampleN + gradientN (device pointers)", "points_per_step": n},
+            "cpu_baseline": base, "gpu_launches": 2 * max(args.steps, 100), "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -822,6 +915,10 @@ def main(argv=None):
         run_hits(args)
     elif args.workload == "surrogate":
         run_surrogate(args)
+    elif args.workload == "render":
+        run_render(args)
+    elif args.workload == "config1":
+        run_config1(args)
     else:
         run_cuda(args)
 

@@ -14,8 +14,14 @@
 //   VKL_CUDA_INTERVAL_ITERATOR_SIZE / VKL_CUDA_HIT_ITERATOR_SIZE instead of
 //   vklGet*IteratorSize. The reference's GPU device publishes its
 //   VKL_MAX_*_ITERATOR_SIZE the same way (max_iterator_size.h).
-// Feature flags are accepted but not needed: the functions dispatch on the
-// volume's type at run time.  `time` is ignored (no temporal formats).
+// Feature flags (vklGetFeatureFlags: the reference's bit layout,
+// VKLFeatureFlagsInternal.h) name the volume types and sample / gradient
+// filters a sampling call may meet; vklComputeSample / SampleM / Gradient
+// skip the excluded paths, and drop them from the inlined code when the
+// argument is a compile-time constant.  VKL_FEATURE_FLAGS_DEFAULT (all bits)
+// and 0 keep every path.  Results are identical either way.  The iterators
+// accept the flags and do not need them.  `time` is ignored (no temporal
+// formats).
 //
 // Results are bit-identical to the host API's when the including
 // translation unit is compiled like the library: nvcc -gencode
@@ -45,6 +51,79 @@ static_assert(sizeof(HitIteratorState) <= VKL_CUDA_HIT_ITERATOR_SIZE, "hit itera
 
 __device__ __forceinline__ f3 toF3(const vkl_vec3f *v) { return {v->x, v->y, v->z}; }
 
+constexpr VKLFeatureFlags kStructuredRegular = 1ull << 0, kVdb = 1ull << 5;
+constexpr VKLFeatureFlags kSampleNearest = 1ull << 6, kSampleLinear = 1ull << 7, kSampleCubic = 1ull << 8;
+constexpr VKLFeatureFlags kGradientNearest = 1ull << 9, kGradientLinear = 1ull << 10, kGradientCubic = 1ull << 11;
+
+// Runs f(field) with the sampler's field type, over the volume kinds the
+// flags allow (the type dispatch of sampleIndexAny).
+template <class F>
+__device__ __forceinline__ auto withField(const DevGrid &g, uint32_t attr, uint32_t depth, VKLFeatureFlags ff, F &&f)
+{
+  const bool denseOk = ff & kStructuredRegular, vdbOk = ff & kVdb;
+  const uint32_t t   = g.type[attr];
+  if (denseOk && (g.dense || !vdbOk)) {
+    switch (t) {
+    case kUChar:
+      return f(DenseField<uint8_t>(g, attr));
+    case kShort:
+      return f(DenseField<int16_t>(g, attr));
+    case kUShort:
+      return f(DenseField<uint16_t>(g, attr));
+    case kHalf:
+      return f(DenseField<__half>(g, attr));
+    case kDouble:
+      return f(DenseField<double>(g, attr));
+    default:
+      return f(DenseField<float>(g, attr));
+    }
+  }
+  switch (g.compress) {
+  case kCompressFP16:
+    return f(SparseField<CodeFP16>(g, attr, depth));
+  case kCompressBF16:
+    return f(SparseField<CodeBF16>(g, attr, depth));
+  case kCompressFP8:
+    return f(SparseField<CodeE4M3>(g, attr, depth));
+  default:
+    break;
+  }
+  if (t == kHalf)
+    return f(SparseField<__half>(g, attr, depth));
+  return f(SparseField<float>(g, attr, depth));
+}
+
+__device__ __forceinline__ float sample(const DevGrid &g, int filter, uint32_t depth, uint32_t attr, f3 oc,
+                                        VKLFeatureFlags ff)
+{
+  if (ff == 0)
+    ff = ~0ull;
+  const f3 p    = xfmPoint(g.objectToIndex, oc);
+  const bool cc = g.constantCellData != 0;
+  return withField(g, attr, depth, ff, [&](const auto &F) -> float {
+    if ((ff & kSampleNearest) && filter == kFilterNearest)
+      return sampleNearest(F, cc, p);
+    if ((ff & kSampleCubic) && filter == kFilterCubic)
+      return sampleCubic(F, p);
+    return sampleLinear(F, p);
+  });
+}
+
+__device__ __forceinline__ f3 gradient(const DevSamplerState *st, uint32_t attr, f3 oc, VKLFeatureFlags ff)
+{
+  if (ff == 0)
+    ff = ~0ull;
+  const DevGrid &g = st->g;
+  const int filter = st->s.gradientFilter;
+  if ((ff & kGradientNearest) && filter == kFilterNearest)
+    return {0.f, 0.f, 0.f};
+  const f3 p = xfmPoint(g.objectToIndex, oc);
+  return withField(g, attr, st->s.maxSamplingDepth, ff, [&](const auto &F) -> f3 {
+    const f3 gi = ((ff & kGradientCubic) && filter == kFilterCubic) ? gradientCubic(F, p) : gradientLinear(F, p);
+    return xfmNormal(g.objectToIndex, gi);
+  });
+}
+
 }  // namespace device_api
 }  // namespace vklcuda
 
@@ -54,10 +133,9 @@ __device__ inline float vklComputeSample(const VKLSampler *sampler, const vkl_ve
                                          const VKLFeatureFlags featureFlags)
 {
   (void)time;
-  (void)featureFlags;
   const auto *st = (const vklcuda::DevSamplerState *)sampler->device;
-  return vklcuda::sampleObjectAny(st->g, st->s.filter, attributeIndex, st->s.maxSamplingDepth,
-                                  vklcuda::device_api::toF3(objectCoordinates));
+  return vklcuda::device_api::sample(st->g, st->s.filter, st->s.maxSamplingDepth, attributeIndex,
+                                     vklcuda::device_api::toF3(objectCoordinates), featureFlags);
 }
 
 // Samples of M attributes (vklComputeSampleM).
@@ -75,11 +153,9 @@ __device__ inline vkl_vec3f vklComputeGradient(const VKLSampler *sampler, const 
                                                const VKLFeatureFlags featureFlags)
 {
   (void)time;
-  (void)featureFlags;
-  const auto *st      = (const vklcuda::DevSamplerState *)sampler->device;
-  const vklcuda::f3 r = vklcuda::gradientObjectAny(st->g, st->s.gradientFilter, attributeIndex,
-                                                   st->s.maxSamplingDepth,
-                                                   vklcuda::device_api::toF3(objectCoordinates));
+  const vklcuda::f3 r = vklcuda::device_api::gradient((const vklcuda::DevSamplerState *)sampler->device,
+                                                      attributeIndex, vklcuda::device_api::toF3(objectCoordinates),
+                                                      featureFlags);
   return vkl_vec3f{r.x, r.y, r.z};
 }
 
@@ -132,11 +208,13 @@ __device__ inline VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext 
 
 __device__ inline int vklIterateHit(VKLHitIterator iterator, VKLHit *hit, const VKLFeatureFlags featureFlags)
 {
-  (void)featureFlags;
   auto *s                   = (vklcuda::device_api::HitIteratorState *)iterator;
   const auto *c             = s->ctx;
   const vklcuda::DevGrid &g = c->sampler->g;
   vklcuda::DevHit h;
+  (void)featureFlags;
+  // the march samples through the generic sampler, out of line (one copy
+  // for every sampling site of the march and bisection)
   if (!vklcuda::hitNext(g, c->sampler->s.filter, c->attr, vklcuda::kNumLevels - 1, c->vr, c->numValues,
                         c->values, s->h, h))
     return 0;

@@ -38,10 +38,14 @@ RENDERERS = os.path.join(HERE, "renderers", "renderers.cu")
 RENDERERS_LIB = os.path.join(HERE, "libopenvkl_renderers.so")
 
 
+INCLUDE = os.path.join(HERE, "..", "include")
+
+
 def _headers():
-    inc = os.path.join(HERE, "..", "include")
+    """Headers the library's translation units include (the __device__ API
+    header is only the renderers')."""
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] + [
-        os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
+        os.path.join(INCLUDE, "openvkl_cuda.h")]
 
 
 def _stale(target, deps):
@@ -66,10 +70,26 @@ def _compile(src, force, verbose):
     return obj
 
 
+def _compile_renderers(force, verbose):
+    obj = os.path.join(OBJ, "renderers.cu.o")
+    if not force and not _stale(obj, [RENDERERS, os.path.join(INCLUDE, "openvkl_cuda_device.h")] + _headers()):
+        return obj
+    cmd = [NVCC] + ARCH + FLAGS + ["-x", "cu", "-c", RENDERERS, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for renderers.cu:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        # the renderer object (the slowest translation unit) compiles beside the library's
+        rend = ex.submit(_compile_renderers, force, verbose)
         objs = list(ex.map(lambda s: _compile(s, force, verbose), SOURCES))
+        robj = rend.result()
     if force or _stale(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
         if verbose:
@@ -77,14 +97,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    if force or _stale(RENDERERS_LIB, [RENDERERS] + _headers()):
-        cmd = [NVCC] + ARCH + FLAGS + ["-shared", "-o", RENDERERS_LIB, RENDERERS, "-lcudart_static", "-lrt",
-                                       "-lpthread", "-ldl"]
+    if force or _stale(RENDERERS_LIB, [robj]):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", RENDERERS_LIB, robj, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed for renderers.cu:\n{r.stdout}\n{r.stderr}")
+            raise RuntimeError(f"link failed for the renderers:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

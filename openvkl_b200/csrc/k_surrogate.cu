@@ -148,10 +148,15 @@ __device__ __forceinline__ void unitPosition(const Encoding &E, f3 p, float u[3]
 }
 
 // Encodes one point into 32 FP16 features (out: 16 half2 slots).
+// UNROLL levels are encoded at once: all 16 (128 table gathers in flight per
+// thread) in inference, 2 in training, whose kernel needs the registers for
+// its backward pass (measured: full unrolling speeds inference 1.9x and
+// slows training 1.2x).
+template <int UNROLL>
 __device__ __forceinline__ void encodePoint(const Encoding &E, const __half2 *__restrict__ table, const float u[3],
                                             __half2 *out)
 {
-#pragma unroll 2
+#pragma unroll UNROLL
   for (int l = 0; l < kLv; ++l) {
     uint32_t i[3];
     float f[3];
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(kThr) kSurrogateInfer(const __grid_constant__ 
       p = {__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2)};
       float u[3];
       unitPosition(E, p, u);
-      encodePoint(E, table, u, row);
+      encodePoint<kLv>(E, table, u, row);
     } else {
       for (int k = 0; k < kLv; ++k)
         row[k] = __floats2half2_rn(0.f, 0.f);
@@ -484,7 +489,7 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
     if (i < n) {
       const f3 p = {__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2)};
       unitPosition(E, p, u);
-      encodePoint(E, table, u, row);
+      encodePoint<2>(E, table, u, row);
     } else {
       for (int k = 0; k < kLv; ++k)
         row[k] = __floats2half2_rn(0.f, 0.f);

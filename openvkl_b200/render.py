@@ -43,7 +43,7 @@ class TransferFunction(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("attributeIndex", C.c_uint), ("time", C.c_float),
-                ("bounds", C.c_float * 6), ("samplingRate", C.c_float), ("intervalColorScale", C.c_float),
+                ("featureFlags", C.c_uint64), ("bounds", C.c_float * 6), ("samplingRate", C.c_float), ("intervalColorScale", C.c_float),
                 ("intervalOpacity", C.c_float), ("firstIntervalOnly", C.c_int), ("showIntervalBorders", C.c_int)]
 
 
@@ -60,8 +60,8 @@ def load_library(path: str = LIB_PATH):
         L.vklExampleRender.argtypes = [C.c_int, vkl.VKLObject, vkl.VKLObject, vkl.VKLObject, C.POINTER(Camera),
                                        C.POINTER(TransferFunction), C.POINTER(Params), C.c_void_p, C.c_void_p]
         L.vklExampleSamplePoints.restype = C.c_int
-        L.vklExampleSamplePoints.argtypes = [vkl.VKLObject, C.c_uint64, C.c_void_p, C.c_uint, C.c_void_p,
-                                             C.c_void_p, C.c_void_p]
+        L.vklExampleSamplePoints.argtypes = [vkl.VKLObject, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -121,6 +121,7 @@ def render(renderer, sampler, camera, width, height, tf=None, interval_context=N
         lo, hi = sampler.volume.value_range()
         tf = transfer_function((lo, hi))
     prm = params(width, height, bounds, **kw)
+    prm.featureFlags = sampler.feature_flags()
     if out is None:
         out = torch.empty((height, width, 4), dtype=torch.float32, device="cuda")
     null = vkl.VKLObject(None, None)
@@ -141,7 +142,7 @@ def sample_points(sampler, points, attr=0):
     n = points.shape[0]
     s = torch.empty(n, dtype=torch.float32, device="cuda")
     g = torch.empty((n, 3), dtype=torch.float32, device="cuda")
-    rc = L.vklExampleSamplePoints(sampler.h, n, points.data_ptr(), attr, s.data_ptr(), g.data_ptr(),
+    rc = L.vklExampleSamplePoints(sampler.h, sampler.feature_flags(), n, points.data_ptr(), attr, s.data_ptr(), g.data_ptr(),
                                   torch.cuda.current_stream().cuda_stream)
     if rc != 0:
         raise RuntimeError(f"vklExampleSamplePoints failed: CUDA error {rc}")

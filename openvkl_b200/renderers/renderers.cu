@@ -43,6 +43,7 @@ typedef struct {
   int width, height;
   unsigned int attributeIndex;
   float time;
+  unsigned long long featureFlags;  // the sampler's (vklGetFeatureFlags)
   float bounds[6];  // volume bounding box (lower xyz, upper xyz)
   float samplingRate;                       // ray march iterator
   float intervalColorScale, intervalOpacity;  // interval iterator debug
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) kRayMarch(VKLSampler sampler, VKLInt
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= prm.width * prm.height)
     return;
-  const VKLFeatureFlags ff = 0;
+  const VKLFeatureFlags ff = prm.featureFlags;
   v3 org, dir;
   pixelRay(cam, prm, idx, org, dir);
   const vkl_range1f tRange = intersectBox(org, dir, prm.bounds);
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) kIntervalDebug(VKLIntervalIteratorCo
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= prm.width * prm.height)
     return;
-  const VKLFeatureFlags ff = 0;
+  const VKLFeatureFlags ff = prm.featureFlags;
   v3 org, dir;
   pixelRay(cam, prm, idx, org, dir);
   const vkl_range1f tRange = intersectBox(org, dir, prm.bounds);
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) kHitRenderer(VKLSampler sampler, VKL
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= prm.width * prm.height)
     return;
-  const VKLFeatureFlags ff = 0;
+  const VKLFeatureFlags ff = prm.featureFlags;
   v3 org, dir;
   pixelRay(cam, prm, idx, org, dir);
   const vkl_range1f tRange = intersectBox(org, dir, prm.bounds);
@@ -269,15 +270,16 @@ __global__ void __launch_bounds__(kThreads) kHitRenderer(VKLSampler sampler, VKL
 // User code sampling its own points with the device API: sample and
 // gradient of every point (the per-point analogue of vklComputeSampleN /
 // vklComputeGradientN).
-__global__ void __launch_bounds__(kThreads) kSamplePoints(VKLSampler sampler, uint64_t n, const float *pts,
-                                                          unsigned int attr, float *samples, float *gradients)
+__global__ void __launch_bounds__(kThreads) kSamplePoints(VKLSampler sampler, VKLFeatureFlags featureFlags,
+                                                          uint64_t n, const float *pts, unsigned int attr,
+                                                          float *samples, float *gradients)
 {
   const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
   if (i >= n)
     return;
   const vkl_vec3f p{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
-  samples[i]        = vklComputeSample(&sampler, &p, attr, 0.f, 0);
-  const vkl_vec3f g = vklComputeGradient(&sampler, &p, attr, 0.f, 0);
+  samples[i]        = vklComputeSample(&sampler, &p, attr, 0.f, featureFlags);
+  const vkl_vec3f g = vklComputeGradient(&sampler, &p, attr, 0.f, featureFlags);
   gradients[3 * i]     = g.x;
   gradients[3 * i + 1] = g.y;
   gradients[3 * i + 2] = g.z;
@@ -315,15 +317,17 @@ __attribute__((visibility("default"))) int vklExampleRender(int renderer, VKLSam
   return (int)cudaGetLastError();
 }
 
-// Samples and gradients of n points (device memory) through the device API.
-__attribute__((visibility("default"))) int vklExampleSamplePoints(VKLSampler sampler, uint64_t n, const float *points,
+// Samples and gradients of n points (device memory) through the device API,
+// with the sampler's feature flags (vklGetFeatureFlags).
+__attribute__((visibility("default"))) int vklExampleSamplePoints(VKLSampler sampler, VKLFeatureFlags featureFlags,
+                                                                  uint64_t n, const float *points,
                                                                   unsigned int attr, float *samples,
                                                                   float *gradients, void *stream)
 {
   if (n == 0)
     return 0;
   kSamplePoints<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, (cudaStream_t)stream>>>(
-      sampler, n, points, attr, samples, gradients);
+      sampler, featureFlags, n, points, attr, samples, gradients);
   return (int)cudaGetLastError();
 }
 
