@@ -222,7 +222,7 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
   staged(d, N, 12, pts, 4 * M, out, [&](uint64_t n, const void *din, void *dout) {
     if (M == 1 && binned(d, s, s->s.filter, n, (const float *)din, attrs[0], (float *)dout, false))
       return;
-    launchSample(s->volume->grid, s->s.filter, s->s.maxSamplingDepth, n, (const float *)din, M,
+    launchSample(s->launchGrid(), s->s.filter, s->s.maxSamplingDepth, n, (const float *)din, M,
                  attrs, (float *)dout, d->stream);
   });
 }
@@ -241,7 +241,7 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
   staged(d, N, 12, pts, 12, out, [&](uint64_t n, const void *din, void *dout) {
     if (binned(d, s, s->s.gradientFilter, n, (const float *)din, attr, (float *)dout, true))
       return;
-    launchGradient(s->volume->grid, s->s.gradientFilter, s->s.maxSamplingDepth, n,
+    launchGradient(s->launchGrid(), s->s.gradientFilter, s->s.maxSamplingDepth, n,
                    (const float *)din, attr, (float *)dout, d->stream);
   });
 }
@@ -842,7 +842,7 @@ VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context, const vk
         cudaCheck(cudaMemcpyAsync(d->stageAux.as<uint8_t>() + ss, ray, sizeof(ray),
                                   cudaMemcpyHostToDevice, d->stream),
                   "iterator init");
-        launchHitIterInit(c->sampler->volume->grid, c->attr, c->depth,
+        launchHitIterInit(c->sampler->launchGrid(), c->attr, c->depth,
                           (const float *)(d->stageAux.as<uint8_t>() + ss), d->stageAux.ptr,
                           d->stream);
         cudaCheck(cudaMemcpyAsync(h + 1, d->stageAux.ptr, ss, cudaMemcpyDeviceToHost, d->stream),
@@ -870,7 +870,7 @@ int vklIterateHit(VKLHitIterator iterator, VKLHit *hit)
         cudaCheck(cudaMemcpyAsync(base, h + 1, ss, cudaMemcpyHostToDevice, d->stream), "iterate");
         DevHit *dOut = (DevHit *)(base + ((ss + 15) & ~size_t(15)));
         int *dRes    = (int *)(dOut + 1);
-        launchHitIterNext(c->sampler->volume->grid, c->sampler->s.filter, c->devValueRanges(),
+        launchHitIterNext(c->sampler->launchGrid(), c->sampler->s.filter, c->devValueRanges(),
                           (uint32_t)c->values.size(), c->devValues.as<float>(), base, dOut, dRes,
                           d->stream);
         struct {
@@ -951,7 +951,7 @@ void vklIterateHitsN(const VKLHitIteratorContext *context, unsigned int N,
       return;
     const bool dev = isDevicePtr(origins) && isDevicePtr(directions) && isDevicePtr(tRanges) &&
                      isDevicePtr(counts) && (maxPerRay == 0 || isDevicePtr(hits));
-    const DevGrid &g = c->sampler->volume->grid;
+    const DevGrid g = c->sampler->launchGrid();
     const int filter = c->sampler->s.filter;
     if (dev) {
       launchHits(g, c->attr, filter, c->depth, c->devValueRanges(), (uint32_t)c->values.size(),
@@ -1013,9 +1013,24 @@ VKLObserver vklNewSamplerObserver(VKLSampler sampler, const char *type)
   return guarded(
       deviceOf(sampler),
       [&]() -> VKLObserver {
-        objectAs<Sampler>(sampler, "sampler");
-        fail(std::string("unsupported sampler observer type '") + (type ? type : "") + "'",
-             VKL_INVALID_ARGUMENT);
+        Sampler *s          = objectAs<Sampler>(sampler, "sampler");
+        const std::string t = type ? type : "";
+        // VdbSampler::newObserver (VdbSampler.cpp:280-290): LeafNodeAccess on
+        // vdb volumes; a uint32 per leaf, set to 1 where sampling reached it
+        if (t != "LeafNodeAccess" || s->volume->isDense)
+          fail("unsupported sampler observer type '" + t + "'", VKL_INVALID_ARGUMENT);
+        if (s->leafObservers.size() >= kMaxLeafObservers)
+          fail("too many LeafNodeAccess observers on one sampler", VKL_INVALID_OPERATION);
+        Observer *o    = new Observer();
+        o->device      = s->device;
+        o->sampler     = Ref<Sampler>(s);
+        o->kind        = t;
+        o->numElements = s->volume->grid.numLeaves;
+        o->devCounters.alloc(std::max<size_t>(4, o->numElements * 4));
+        cudaCheck(cudaMemset(o->devCounters.ptr, 0, o->devCounters.bytes), "memset");
+        s->leafObservers.push_back(o);
+        s->uploadState();
+        return handleOf(o);
       },
       VKLObserver{nullptr, nullptr});
 }
@@ -1027,7 +1042,9 @@ const void *vklMapObserver(VKLObserver observer)
       [&]() -> const void * {
         Observer *o = objectAs<Observer>(observer, "observer");
         o->commit();
-        return o->buffer.data();
+        if (o->kind == "LeafNodeAccess")
+          return (const void *)o->leafAccess.data();
+        return (const void *)o->buffer.data();
       },
       (const void *)nullptr);
 }
@@ -1039,8 +1056,7 @@ VKLDataType vklGetObserverElementType(VKLObserver observer)
   return guarded(
       deviceOf(observer),
       [&]() -> VKLDataType {
-        objectAs<Observer>(observer, "observer");
-        return VKL_OBJECT;
+        return objectAs<Observer>(observer, "observer")->kind == "LeafNodeAccess" ? VKL_UINT : VKL_OBJECT;
       },
       VKL_UNKNOWN);
 }
@@ -1049,7 +1065,10 @@ size_t vklGetObserverElementSize(VKLObserver observer)
 {
   return guarded(
       deviceOf(observer),
-      [&]() -> size_t { return objectAs<Observer>(observer, "observer")->elementFloats * 4; },
+      [&]() -> size_t {
+        const Observer *o = objectAs<Observer>(observer, "observer");
+        return o->kind == "LeafNodeAccess" ? sizeof(uint32_t) : o->elementFloats * 4;
+      },
       (size_t)0);
 }
 

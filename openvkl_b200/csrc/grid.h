@@ -108,6 +108,8 @@ enum : uint32_t {
   kCompressFP8  = 3,
 };
 
+constexpr uint32_t kMaxLeafObservers = 4;
+
 struct DevGrid {
   float objectToIndex[12];
   float indexToObject[12];
@@ -140,6 +142,11 @@ struct DevGrid {
   // memory budget; the walk is used then, and for maxSamplingDepth < 3.
   const uint64_t *leafMap;
   uint32_t leafMapDims[3];
+  // LeafNodeAccess observers of the sampler a launch runs for (sparse only):
+  // every traversal that reaches a leaf sets leafAccess[i][leaf] = 1, like
+  // VdbLeafAccessObserver_observe (unsynchronised stores of the same value).
+  uint32_t numLeafAccess;
+  uint32_t *leafAccess[kMaxLeafObservers];
 };
 
 struct DevSampler {

@@ -897,8 +897,23 @@ void Sampler::commit()
   for (int f : {s.filter, s.gradientFilter})
     if (f != kFilterNearest && f != kFilterLinear && f != kFilterCubic)
       fail("invalid filter");
+  uploadState();
+}
+
+DevGrid Sampler::launchGrid() const
+{
+  DevGrid g       = volume->grid;
+  g.numLeafAccess = 0;
+  for (Observer *o : leafObservers)
+    if (g.numLeafAccess < kMaxLeafObservers)
+      g.leafAccess[g.numLeafAccess++] = o->devCounters.as<uint32_t>();
+  return g;
+}
+
+void Sampler::uploadState()
+{
   // the handle's device pointer stays valid across commits: allocate once
-  const DevSamplerState state{volume->grid, s};
+  const DevSamplerState state{launchGrid(), s};
   if (!devState.ptr)
     devState.alloc(sizeof(state));
   cudaCheck(cudaMemcpy(devState.ptr, &state, sizeof(state), cudaMemcpyHostToDevice), "upload");
@@ -1012,8 +1027,29 @@ DevValueRanges HitContext::devValueRanges() const
 // and value ranges of all leaf-pointer voxels and of non-empty voxels at
 // maxDepth, read back from the device tree.
 // ---------------------------------------------------------------------------
+Observer::~Observer()
+{
+  if (kind == "LeafNodeAccess" && sampler) {
+    auto &v = sampler->leafObservers;
+    v.erase(std::remove(v.begin(), v.end(), this), v.end());
+    try {
+      sampler->uploadState();
+    } catch (...) {
+    }
+  }
+}
+
 void Observer::commit()
 {
+  if (kind == "LeafNodeAccess") {
+    // VdbLeafAccessObserver::map: the buffer as the sampling left it
+    leafAccess.resize(numElements);
+    cudaCheck(cudaStreamSynchronize(device->stream), "observer");
+    if (numElements)
+      cudaCheck(cudaMemcpy(leafAccess.data(), devCounters.ptr, numElements * 4, cudaMemcpyDeviceToHost),
+                "observer readback");
+    return;
+  }
   buffer.clear();
   numElements = 0;
   if (kind == "InnerNode") {

@@ -271,12 +271,21 @@ struct Volume : ManagedObject {
   void finishCommit(const float indexLo[3], const float indexHi[3]);
 };
 
+struct Observer;
+
 struct Sampler : ManagedObject {
   Ref<Volume> volume;
   DevSampler s{};
   DeviceBuffer devState;  // DevSamplerState for the device-side API
+  // LeafNodeAccess observers (VdbSampler::newObserver); each removes itself
+  // when released.
+  std::vector<Observer *> leafObservers;
   const char *typeName() const override { return "Sampler"; }
   void commit() override;
+  // The volume's grid with this sampler's observer buffers: what its
+  // sampling and hit-iteration launches read.
+  DevGrid launchGrid() const;
+  void uploadState();
 };
 
 struct IntervalContext : ManagedObject {
@@ -314,8 +323,9 @@ struct Observer : ManagedObject {
   std::vector<float> buffer;
   size_t elementFloats = 0;
   size_t numElements   = 0;
-  std::vector<uint32_t> leafAccess;  // LeafNodeAccess counters (host copy)
-  DeviceBuffer devCounters;
+  std::vector<uint32_t> leafAccess;  // LeafNodeAccess buffer (host copy at map)
+  DeviceBuffer devCounters;          // LeafNodeAccess buffer, one uint32 per leaf
+  ~Observer() override;
   const char *typeName() const override { return "Observer"; }
   void commit() override;
 };

@@ -298,10 +298,16 @@ struct SparseField {
   // offset: one load from the flat leaf map at full depth, else the walk.
   __device__ __forceinline__ uint64_t traverse(uint32_t ox, uint32_t oy, uint32_t oz) const
   {
-    if (g.leafMap && maxDepth >= kNumLevels - 1)
-      return __ldg(g.leafMap + ((uint64_t)(oz >> 3) * g.leafMapDims[1] + (oy >> 3)) * g.leafMapDims[0] +
-                   (ox >> 3));
-    return walk(ox, oy, oz);
+    const uint64_t v =
+        (g.leafMap && maxDepth >= kNumLevels - 1)
+            ? __ldg(g.leafMap + ((uint64_t)(oz >> 3) * g.leafMapDims[1] + (oy >> 3)) * g.leafMapDims[0] + (ox >> 3))
+            : walk(ox, oy, oz);
+    // LeafNodeAccess observers (VdbSampleInner.ih.in:68-74): a reached leaf
+    // (not an empty or depth-limited voxel) is marked in every buffer
+    if (g.numLeafAccess && voxelIsLeaf(v))
+      for (uint32_t i = 0; i < g.numLeafAccess; ++i)
+        g.leafAccess[i][voxelLeafIndex(v)] = 1u;
+    return v;
   }
 
   // Walk from the root to the voxel holding the leaf that contains the

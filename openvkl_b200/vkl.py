@@ -422,9 +422,19 @@ class Volume(_Obj):
 
 
 class VKLObserverObj(_Obj):
-    def __init__(self, device, handle):
+    def __init__(self, device, handle, what="vklNewVolumeObserver"):
         super().__init__(device, handle)
-        self._check_handle("vklNewVolumeObserver")
+        self._check_handle(what)
+
+    def read_uint(self):
+        """The mapped buffer of a uint32 observer (LeafNodeAccess)."""
+        p = self._call(self.lib.vklMapObserver, self.h)
+        n = self.lib.vklGetObserverNumElements(self.h)
+        if n == 0:
+            return np.zeros(0, np.uint32)
+        out = np.array((C.c_uint32 * n).from_address(p), np.uint32)
+        self.lib.vklUnmapObserver(self.h)
+        return out
 
     def read(self):
         p = self.lib.vklMapObserver(self.h)
@@ -668,6 +678,13 @@ class Sampler(_Obj):
 
     def feature_flags(self):
         return self.lib.vklGetFeatureFlags(self.h)
+
+    def leaf_access_observer(self):
+        """vklNewSamplerObserver(sampler, "LeafNodeAccess"); read with .read_uint()."""
+        self.device.pending = None
+        h = self.lib.vklNewSamplerObserver(self.h, b"LeafNodeAccess")
+        self.device.raise_pending()
+        return VKLObserverObj(self.device, h, "vklNewSamplerObserver")
 
     def sample(self, points, attr=0, out=None):
         n = points.shape[0]

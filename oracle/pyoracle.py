@@ -81,6 +81,7 @@ def lib(fast: bool = False) -> C.CDLL:
         L.orc_sample.argtypes = [P, C.c_int, U32, U64, P, U32, P]
         L.orc_gradient.argtypes = [P, C.c_int, U32, U64, P, U32, P]
         L.orc_sample_parallel.argtypes = [P, C.c_int, U64, P, U32, P, C.c_int]
+        L.orc_sample_observed.argtypes = [P, C.c_int, U32, U64, P, U32, P, P]
         L.orc_sample_fp64.argtypes = [P, C.c_int, U64, P, U32, P]
         L.orc_iterate_intervals.argtypes = [P, U32, U32, P, F32, U64, P, P, P, U32, P, P]
         L.orc_iterate_hits.argtypes = [P, U32, C.c_int, U32, P, U64, P, P, P, U32, P, P]
@@ -202,6 +203,15 @@ class OracleVolume:
         out = np.zeros(len(pts), np.float32)
         self._lib.orc_sample(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out))
         return out
+
+    def sample_observed(self, points, num_leaves, filter=FILTER_LINEAR, attr=0, max_sampling_depth=3):
+        """(samples, LeafNodeAccess buffer: uint32 per leaf, 1 where a walk reached it)."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.empty(len(pts), np.float32)
+        acc = np.zeros(num_leaves, np.uint32)
+        self._lib.orc_sample_observed(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out),
+                                      _p(acc))
+        return out, acc
 
     def sample_parallel(self, points, filter=FILTER_LINEAR, attr=0, threads=0):
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)

@@ -347,8 +347,13 @@ inline float traverseAndSampleDense(const Grid &g, const vec3i &ic, uint32_t a)
   return g.background[a];
 }
 
+// LeafNodeAccess observer buffer of the sampling call in progress (set by
+// orc_sample_observed only): the walk marks every leaf it reaches.
+thread_local uint32_t *t_leafAccess = nullptr;
+
 // Tree walk (VdbSampler_traverse, VdbSampler_traverseAndSample.ih:85-146,
-// VdbSampleInner.ih.in:33-76): returns the leaf / error / empty voxel.
+// VdbSampleInner.ih.in:33-76): returns the leaf / error / empty voxel; a
+// reached leaf is observed as VdbSampleInner.ih.in:68-74 does.
 inline uint64_t traverse(const Grid &g,
                          const vec3ui &domainOffset,
                          uint32_t maxSamplingDepth)
@@ -367,6 +372,8 @@ inline uint64_t traverse(const Grid &g,
       node = childIdx(v);
       continue;
     }
+    if (t_leafAccess && vLeaf(v))
+      t_leafAccess[leafIdx(v)] = 1;
     return v;
   }
   return 0;
@@ -1543,6 +1550,14 @@ void orc_sample(const OrcVolume *v, int filter, uint32_t depth, uint64_t n, cons
     const vec3f p = xfmPoint(g.o2i, {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]});
     out[i]        = sampleAt(g, filter, p, attr, depth);
   }
+}
+
+void orc_sample_observed(const OrcVolume *v, int filter, uint32_t depth, uint64_t n, const float *pts,
+                         uint32_t attr, float *out, uint32_t *leafAccess)
+{
+  t_leafAccess = leafAccess;
+  orc_sample(v, filter, depth, n, pts, attr, out);
+  t_leafAccess = nullptr;
 }
 
 void orc_sample_parallel(const OrcVolume *v, int filter, uint64_t n, const float *pts,

@@ -97,6 +97,10 @@ void orc_gradient(const OrcVolume *v,
                   const float *points,
                   uint32_t attr,
                   float *out);
+// orc_sample with a LeafNodeAccess observer buffer (one uint32 per leaf):
+// every leaf a tap's tree walk reaches is set to 1 (VdbLeafAccessObserver.ih).
+void orc_sample_observed(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint64_t n,
+                         const float *points, uint32_t attr, float *out, uint32_t *leafAccess);
 // Same as orc_sample but split over `threads` OpenMP threads (CPU baseline).
 void orc_sample_parallel(const OrcVolume *v,
                          int filter,

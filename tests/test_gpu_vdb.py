@@ -127,3 +127,41 @@ def test_vdb_validation_errors(vkl, device):
     assert e.value.code == 1 and e.value.msg == "invalid node level 4 for this vdb configuration"
     with pytest.raises(vkl.VKLError, match="Node data too small"):
         vkl.vdb_volume(device, [3], [[0, 0, 0]], [1], node_data=[data[:1]])
+
+
+@pytest.mark.parametrize("fv,depth", [(0, 3), (100, 3), (200, 3), (100, 1)])
+def test_leaf_access_observer(vkl, device, oracle, fv, depth):
+    """vklNewSamplerObserver(sampler, "LeafNodeAccess"): after sampling, the
+    observer's buffer (one uint32 per leaf) holds 1 exactly at the leaves
+    the oracle's tree walks reached (VdbSampleInner.ih.in:68-74), including
+    tiles and excluding voxels the maxSamplingDepth cut stops above."""
+    origins, levels, formats, vals, tvals = _shell_vdb()
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tvals)
+    smp = vkl.Sampler(vol, filter=fv, max_sampling_depth=depth)
+    obs = smp.leaf_access_observer()
+    assert not obs.read_uint().any()
+    rng = np.random.default_rng(11)
+    n_leaves = len(vals) // 512
+    pts = (origins[:n_leaves][rng.integers(0, n_leaves, 3000)] + rng.uniform(-2, 10, (3000, 3))).astype(np.float32)
+    b = ref.info()["bounds"]
+    pts = np.concatenate([pts, uniform_points(2000, b[:3] - 4, b[3:] + 4, seed=12)])
+    smp.sample(pts)
+    got = obs.read_uint()
+    want_s, want = ref.sample_observed(pts, len(got), filter=fv, max_sampling_depth=depth)
+    np.testing.assert_array_equal(got, want)
+    if depth == 3:
+        assert got.any()
+    # a second observer records only what is sampled after it exists
+    obs2 = smp.leaf_access_observer()
+    smp.sample(pts[:50])
+    _, want2 = ref.sample_observed(pts[:50], len(got), filter=fv, max_sampling_depth=depth)
+    np.testing.assert_array_equal(obs2.read_uint(), want2)
+    obs.release()
+    np.testing.assert_array_equal(bits(smp.sample(pts)), bits(want_s))
+
+
+def test_leaf_access_observer_needs_a_vdb_volume(vkl, device):
+    vol = vkl.structured_regular(device, sinusoid_field((16, 16, 16), seed=1))
+    with pytest.raises(vkl.VKLError, match="unsupported sampler observer type"):
+        vkl.Sampler(vol).leaf_access_observer()
