@@ -46,7 +46,7 @@ UNIT = "Gsamples/s"
 MAX_CPU_POINTS = 1 << 27  # bounded CPU sample (1.6 GB of points)
 FILTER = {"coherent": 100, "incoherent": 100, "cubic": 200, "gradient": 100, "vdb": 100, "batched": 100,
           "intervals": 100, "hits": 100, "surrogate": 100,
-          "render": 100, "config1": 100, "vdb_coherent": 100}
+          "render": 100, "config1": 100, "vdb_coherent": 100, "commit": 100}
 BATCH_VOLUMES = 512
 VDB_DOMAIN, VDB_POINTS = 4096, 1 << 26
 HIT_RAYS = 1 << 24
@@ -897,6 +897,113 @@ def run_config1(args):
     print(json.dumps(line), flush=True)
 
 
+def run_commit(args):
+    """vklCommit of the 1024^3 float32 structuredRegular volume: the bricked
+    re-layout, the dense tree, the per-leaf value ranges over 10^3 voxel
+    windows, their propagation up the tree and the volume range read back
+    (DenseVdbVolume.cpp:21-119 with VdbVolume.cpp:338-392).  Unit:
+    Gvoxels/s.  Device-resident voxels (VKL_DATA_SHARED_BUFFER) for `value`;
+    `e2e` hands the voxels over from pinned host memory (vklNewData copies
+    them) and reads the value range back.  Each commit is timed alone with
+    events on the device stream; the release of the previous volume is
+    outside the timed region.  CPU baseline: the oracle's commit of a 256^3
+    volume of the same field."""
+    import torch
+    from openvkl_b200 import vkl
+    torch.cuda.set_device(0)
+    dev = vkl.Device("cuda")
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    vox = volume_numpy()
+    tvox = torch.from_numpy(vox).cuda()
+    nvox = vox.size
+    leaves = math.prod((d + 7) // 8 for d in DIMS)
+
+    def timed_commits(make, steps):
+        ts = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            v = make()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            if v is not None:
+                v.release()
+            del v
+        return ts
+
+    timed_commits(lambda: vkl.structured_regular(dev, tvox, shared=True), args.warmup)
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        ts = timed_commits(lambda: vkl.structured_regular(dev, tvox, shared=True), args.steps)
+    ms = sum(ts) / len(ts)
+    lo, hi = (float(x) for x in vkl.structured_regular(dev, tvox, shared=True).value_range())
+
+    # a time-varying volume: the same object re-committed with a new data
+    # object each step (its device buffers are reused)
+    vol = vkl.structured_regular(dev, tvox, shared=True)
+
+    def recommit():
+        vol._keep.clear()
+        vol.set_data("data", vkl.Data(dev, tvox, shared=True))
+        vol.commit()
+    timed_commits(recommit, args.warmup)
+    rts = timed_commits(recommit, args.steps)
+    del vol
+
+    e2e = None
+    if not args.no_extras:
+        host = torch.from_numpy(vox).pin_memory()
+
+        def from_host():
+            v = vkl.structured_regular(dev, host)
+            v.value_range()
+            return v
+        from_host().release()
+        t = timed_commits(from_host, min(args.steps, 5))
+        e2e = {"value": nvox / (sum(t) / len(t) * 1e-3) / 1e9, "unit": "Gvoxels/s",
+               "h2d_bytes_per_step": nvox * 4, "d2h_bytes_per_step": 8}
+        del host
+
+    # bricked copy (4 B read + 4 B written per voxel), leaf ranges (4 B read
+    # per voxel, 8 B written per leaf)
+    alg = nvox * 12 + leaves * 8
+    peak, peak_kind = peaks()
+    base = None
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        svox = volume_numpy((256, 256, 256))
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            O.OracleVolume.dense_volume(svox, fast=True)
+            reps += 1
+            dt = time.perf_counter() - t0
+            if dt > 10.0 or reps >= 20:
+                break
+        base = {"value": reps * svox.size / dt / 1e9, "unit": "Gvoxels/s", "cores": 1, "kind": "port",
+                "sample": f"{reps} commits of a 256^3 volume of the same field; oracle C++ restatement of the "
+                          f"reference's dense commit and value-range builder, one host thread, {dt:.1f} s"}
+    line = {"metric": "commit Gvoxels/s (value-range builder)", "value": nvox / (ms * 1e-3) / 1e9,
+            "unit": "Gvoxels/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "ms_per_step_all": ts, "recommit_ms_median": statistics.median(rts), "recommit_ms_all": rts,
+            "recommit_gvoxels_s_median": nvox / (statistics.median(rts) * 1e-3) / 1e9,
+            "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded sinusoid volume)",
+            "config": {"workload": "vklCommit of a structuredRegular 1024^3 float32 volume (bricked re-layout, "
+                                   "dense tree, leaf value ranges, propagation, volume range readback)",
+                       "voxels": nvox, "leaves": leaves, "value_range": [lo, hi],
+                       "l2": "4 GiB volume, larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg, "traffic": None,
+                         "note": "whole commit (several kernels, allocations and one readback)"},
+            "cpu_baseline": base, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -936,6 +1043,8 @@ def main(argv=None):
         run_config1(args)
     elif args.workload == "vdb_coherent":
         run_vdb_coherent(args)
+    elif args.workload == "commit":
+        run_commit(args)
     else:
         run_cuda(args)
 

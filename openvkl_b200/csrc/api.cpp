@@ -480,14 +480,21 @@ VKLData vklNewData(VKLDevice dev, size_t numItems, VKLDataType type, const void 
                       "data copy");
           cudaCheck(cudaStreamSynchronize(d->stream), "data copy");
           data->dev = data->owned.ptr;
+        } else if (stride == isz) {
+          // compact host source: uploaded from the caller's memory (a DMA
+          // when it is pinned); small arrays also keep a host copy
+          data->owned.alloc(bytes);
+          cudaCheck(cudaMemcpyAsync(data->owned.ptr, source, bytes, cudaMemcpyHostToDevice, d->stream),
+                    "data upload");
+          if (bytes <= (64u << 20))
+            data->host.assign((const uint8_t *)source, (const uint8_t *)source + bytes);
+          cudaCheck(cudaStreamSynchronize(d->stream), "data upload");
+          data->dev = data->owned.ptr;
         } else {
-          // host source: compact host copy (kept for small arrays) + device copy
+          // strided host source: compacted on the host first
           std::vector<uint8_t> compact(bytes);
-          if (stride == isz)
-            std::memcpy(compact.data(), source, bytes);
-          else
-            for (size_t i = 0; i < numItems; ++i)
-              std::memcpy(&compact[i * isz], (const uint8_t *)source + i * stride, isz);
+          for (size_t i = 0; i < numItems; ++i)
+            std::memcpy(&compact[i * isz], (const uint8_t *)source + i * stride, isz);
           data->owned.alloc(bytes);
           cudaCheck(cudaMemcpy(data->owned.ptr, compact.data(), bytes, cudaMemcpyHostToDevice),
                     "data upload");

@@ -80,52 +80,204 @@ __global__ void kDenseLevel0(uint64_t *vox0, uint3 n1)
 }
 
 // ---------------------------------------------------------------------------
-// Dense leaf ranges.  The reference scans, for each leaf, the voxel windows
-// [7,8) | [0,8) | [0,2) of its 3x3x3 leaf neighbourhood, skipping voxels
-// outside the dense dimensions, and adds the background for neighbours whose
-// origin lies outside the domain (VdbSampler.ispc:460-557,
-// VdbSampler_dense.ih:35-105).  Per axis that is the clipped voxel box
-// [o-1, o+10); the background joins when o-8 < 0 or o+8 >= dims on any axis
-// and is skipped when NaN.  min/max are exact, so the scan order is free.
+// Dense commit: bricked copy and leaf ranges in one pass over the voxels.
 //
-// One thread per (leaf, x-window column): a block covers 32 consecutive
-// leaves along x for one (ly, lz), so a warp's loads along a row are
-// contiguous; the 11x11 (y,z) rows of the window are read through L1/L2.
+// The reference computes, per leaf, the range of each of its 27 neighbour
+// leaves' windows [7,8) | [0,8) | [0,2) per axis, in neighbour order
+// (x, y, z) and, inside a window, voxel order x outer / z inner, each fold
+// being extend() = (a < b ? a : b, a > b ? a : b); a neighbour whose origin
+// lies outside the domain contributes (background, background); a neighbour
+// range whose bound is NaN is skipped (VdbSampler.ispc:460-557,
+// VdbSampler_dense.ih:35-105).  Per axis the union of the windows is the
+// voxel box [o-1, o+10) clipped to the dimensions.
+//
+// Without NaN in the window every order of the folds gives the same value:
+// the min / max over the clipped box, plus the background when some
+// neighbour origin is outside the domain and the background is not NaN.
+// The bits are the same too unless a bound is zero and both +0.0 and -0.0
+// take part.  The kernel computes that separably (x, then y, then z) with
+// per-window flags for NaN and -0.0; a leaf whose window holds a NaN (a NaN
+// voxel resets a running bound, so the order matters), or whose zero bound
+// may come from a -0.0, is recomputed in the reference's own fold order.
+//
+// One CTA owns a column of 4x4 leaves (32x32 voxels) and kDenseChunk leaf
+// layers: it streams the voxel planes z = 8*k0-1 .. 8*k1+1 through shared
+// memory (35x35 with the halo), writes each interior plane to the bricked
+// array, reduces every plane to per-leaf-column (lo, hi, flag), then folds
+// 11 planes per leaf.  Each voxel is read from HBM about once (halo reads
+// hit L2 for the x / y neighbours of concurrently running CTAs).
 // ---------------------------------------------------------------------------
+constexpr int kDenseChunk = 8;              // leaf layers per CTA
+constexpr int kPlaneW     = 35;             // 32 + halo (1 before, 2 after)
+constexpr int kMaxPlanes  = 8 * kDenseChunk + 3;
+
 template <typename T>
-__global__ void __launch_bounds__(256) kDenseLeafRanges(const __grid_constant__ DevGrid g,
-                                                        uint32_t attr, uint3 nl,
-                                                        float *__restrict__ leafRanges)
+__device__ __forceinline__ float toFloat(T v)
 {
-  const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t numLeaves = (uint64_t)nl.x * nl.y * nl.z;
-  if (leaf >= numLeaves)
-    return;
-  const uint32_t lx = (uint32_t)(leaf % nl.x), ly = (uint32_t)((leaf / nl.x) % nl.y),
-                 lz = (uint32_t)(leaf / ((uint64_t)nl.x * nl.y));
-  const int32_t X = g.denseDims[0], Y = g.denseDims[1], Z = g.denseDims[2];
-  const int32_t ox = (int32_t)lx * 8, oy = (int32_t)ly * 8, oz = (int32_t)lz * 8;
-  const int32_t x0 = max(ox - 1, 0), x1 = min(ox + 10, X);
-  const int32_t y0 = max(oy - 1, 0), y1 = min(oy + 10, Y);
-  const int32_t z0 = max(oz - 1, 0), z1 = min(oz + 10, Z);
-  const T *data = (const T *)g.data[attr];
+  return (float)v;
+}
+template <>
+__device__ __forceinline__ float toFloat<__half>(__half v)
+{
+  return __half2float(v);
+}
+template <>
+__device__ __forceinline__ float toFloat<double>(double v)
+{
+  return __double2float_rn(v);
+}
+
+// Values for which the fold order can change the bits: NaN (bit 0) and
+// -0.0 (bit 1).
+constexpr uint32_t kFlagNaN = 1u, kFlagNegZero = 2u;
+__device__ __forceinline__ uint32_t orderFlags(float v)
+{
+  return (isnan(v) ? kFlagNaN : 0u) | (__float_as_uint(v) == 0x80000000u ? kFlagNegZero : 0u);
+}
+
+struct PartialRange {
+  float lo, hi;
+  uint32_t flag;
+};
+
+// The reference's fold order for one leaf at voxel origin (ox, oy, oz).
+template <typename T>
+__device__ float2 denseLeafRangeExact(const T *__restrict__ src, uint3 dims, int32_t ox, int32_t oy,
+                                      int32_t oz, float bg)
+{
   float lo = kInf, hi = -kInf;
-  for (int32_t z = z0; z < z1; ++z)
-    for (int32_t y = y0; y < y1; ++y)
-      for (int32_t x = x0; x < x1; ++x) {
-        const float v = ldv(data, brickIndex(x, y, z, g.superX, g.superY));
-        lo            = fminx(lo, v);
-        hi            = fmaxx(hi, v);
+  for (int ix = 0; ix < 3; ++ix)
+    for (int iy = 0; iy < 3; ++iy)
+      for (int iz = 0; iz < 3; ++iz) {
+        const uint32_t nx = (uint32_t)(ox + (ix - 1) * 8), ny = (uint32_t)(oy + (iy - 1) * 8),
+                       nz = (uint32_t)(oz + (iz - 1) * 8);
+        float nlo, nhi;
+        if (!(nx < dims.x && ny < dims.y && nz < dims.z)) {
+          nlo = nhi = bg;
+        } else {
+          nlo = kInf;
+          nhi = -kInf;
+          const uint32_t xa = ix == 0 ? 7 : 0, xb = ix == 2 ? 2 : 8;
+          const uint32_t ya = iy == 0 ? 7 : 0, yb = iy == 2 ? 2 : 8;
+          const uint32_t za = iz == 0 ? 7 : 0, zb = iz == 2 ? 2 : 8;
+          for (uint32_t x = xa; x < xb; ++x)
+            for (uint32_t y = ya; y < yb; ++y)
+              for (uint32_t z = za; z < zb; ++z) {
+                const uint32_t px = nx + x, py = ny + y, pz = nz + z;
+                if (!(px < dims.x && py < dims.y && pz < dims.z))
+                  continue;
+                const float v = toFloat(src[((uint64_t)pz * dims.y + py) * dims.x + px]);
+                nlo           = fminx(nlo, v);
+                nhi           = fmaxx(nhi, v);
+              }
+        }
+        if (!isnan(nlo))
+          lo = fminx(lo, nlo);
+        if (!isnan(nhi))
+          hi = fmaxx(hi, nhi);
       }
-  const bool boundary = ox - 8 < 0 || oy - 8 < 0 || oz - 8 < 0 || ox + 8 >= X || oy + 8 >= Y ||
-                        oz + 8 >= Z;
-  const float bg = g.background[attr];
-  if (boundary && !isnan(bg)) {
-    lo = fminx(lo, bg);
-    hi = fmaxx(hi, bg);
+  return make_float2(lo, hi);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kDenseBrickRanges(const T *__restrict__ src, T *__restrict__ dst,
+                                                         uint3 dims, uint3 nl, uint32_t superX, uint32_t superY,
+                                                         float bg, float *__restrict__ leafRanges)
+{
+  __shared__ T plane[kPlaneW][kPlaneW];
+  __shared__ PartialRange xres[kPlaneW][4];
+  __shared__ PartialRange pres[kMaxPlanes][16];
+  const int tid   = threadIdx.x;
+  const int32_t X0 = 32 * (int32_t)blockIdx.x, Y0 = 32 * (int32_t)blockIdx.y;
+  const int32_t X = (int32_t)dims.x, Y = (int32_t)dims.y, Z = (int32_t)dims.z;
+  const int32_t k0 = kDenseChunk * (int32_t)blockIdx.z, k1 = min(k0 + kDenseChunk, (int32_t)nl.z);
+  const int32_t zBeg = max(8 * k0 - 1, 0), zEnd = min(8 * k1 + 2, Z);
+  // The next plane is loaded into registers while the current one is
+  // reduced, so the loads of one plane overlap the work on the previous.
+  constexpr int kPerThread = (kPlaneW * kPlaneW + 255) / 256;
+  T next[kPerThread];
+  auto loadPlane = [&](int32_t z) {
+    const uint64_t zoff = (uint64_t)z * dims.y;
+#pragma unroll
+    for (int u = 0; u < kPerThread; ++u) {
+      const int e = tid + 256 * u, r = e / kPlaneW, c = e - r * kPlaneW;
+      const int32_t y = Y0 - 1 + r, x = X0 - 1 + c;
+      if (e < kPlaneW * kPlaneW && (uint32_t)x < dims.x && (uint32_t)y < dims.y)
+        next[u] = src[(zoff + y) * dims.x + x];
+    }
+  };
+  loadPlane(zBeg);
+  for (int32_t z = zBeg; z < zEnd; ++z) {
+#pragma unroll
+    for (int u = 0; u < kPerThread; ++u) {
+      const int e = tid + 256 * u;
+      if (e < kPlaneW * kPlaneW)
+        plane[e / kPlaneW][e % kPlaneW] = next[u];
+    }
+    __syncthreads();
+    if (z + 1 < zEnd)
+      loadPlane(z + 1);
+    if (z >= 8 * k0 && z < 8 * k1) {
+      for (int e = tid; e < 1024; e += 256) {
+        const int32_t y = Y0 + (e >> 5), x = X0 + (e & 31);
+        if (x < X && y < Y)
+          dst[brickIndex((uint32_t)x, (uint32_t)y, (uint32_t)z, superX, superY)] = plane[(e >> 5) + 1][(e & 31) + 1];
+      }
+    }
+    if (tid < kPlaneW * 4) {
+      const int r = tid >> 2, i = tid & 3;
+      const int32_t y = Y0 - 1 + r;
+      PartialRange pr{kInf, -kInf, 0u};
+      if ((uint32_t)y < dims.y && X0 + 8 * i < X) {
+        const int c0 = max(8 * i, 1 - X0), c1 = min(8 * i + 11, X - X0 + 1);
+        for (int c = c0; c < c1; ++c) {
+          const float v = toFloat(plane[r][c]);
+          pr.flag |= orderFlags(v);
+          pr.lo = fminf(pr.lo, v);
+          pr.hi = fmaxf(pr.hi, v);
+        }
+      }
+      xres[r][i] = pr;
+    }
+    __syncthreads();
+    if (tid < 16) {
+      const int i = tid & 3, j = tid >> 2;
+      PartialRange pr{kInf, -kInf, 0u};
+      for (int r = 8 * j; r < 8 * j + 11; ++r) {
+        const PartialRange q = xres[r][i];
+        pr.lo = fminf(pr.lo, q.lo);
+        pr.hi = fmaxf(pr.hi, q.hi);
+        pr.flag |= q.flag;
+      }
+      pres[z - zBeg][tid] = pr;
+    }
   }
-  leafRanges[2 * leaf]     = lo;
-  leafRanges[2 * leaf + 1] = hi;
+  __syncthreads();
+  const int layer = tid >> 4, col = tid & 15;
+  const int32_t lx = 4 * (int32_t)blockIdx.x + (col & 3), ly = 4 * (int32_t)blockIdx.y + (col >> 2),
+                lz = k0 + layer;
+  if (layer >= kDenseChunk || lz >= k1 || lx >= (int32_t)nl.x || ly >= (int32_t)nl.y)
+    return;
+  PartialRange pr{kInf, -kInf, 0u};
+  for (int32_t z = max(8 * lz - 1, 0); z < min(8 * lz + 10, Z); ++z) {
+    const PartialRange q = pres[z - zBeg][col];
+    pr.lo = fminf(pr.lo, q.lo);
+    pr.hi = fmaxf(pr.hi, q.hi);
+    pr.flag |= q.flag;
+  }
+  const int32_t ox = 8 * lx, oy = 8 * ly, oz = 8 * lz;
+  const bool boundary = lx == 0 || ly == 0 || lz == 0 || ox + 8 >= X || oy + 8 >= Y || oz + 8 >= Z;
+  float2 r = make_float2(pr.lo, pr.hi);
+  if (boundary && !isnan(bg)) {
+    r.x = fminf(r.x, bg);
+    r.y = fmaxf(r.y, bg);
+    pr.flag |= orderFlags(bg) & kFlagNegZero;
+  }
+  if ((pr.flag & kFlagNaN) || ((pr.flag & kFlagNegZero) && (r.x == 0.f || r.y == 0.f)))
+    r = denseLeafRangeExact(src, dims, ox, oy, oz, bg);
+  const uint64_t leaf = ((uint64_t)lz * nl.y + ly) * nl.x + lx;
+  leafRanges[2 * leaf]     = r.x;
+  leafRanges[2 * leaf + 1] = r.y;
 }
 
 // ---------------------------------------------------------------------------
@@ -371,21 +523,6 @@ __global__ void __launch_bounds__(256) kCompressLeaves(const float *__restrict__
 
 inline unsigned blocksFor(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
-// x-fastest user array -> bricked copy; one thread per voxel, element size
-// only (the layout does not depend on the voxel type).
-template <typename E>
-__global__ void kToBricked(const E *__restrict__ src, E *__restrict__ dst, uint3 dims, uint32_t superX,
-                           uint32_t superY)
-{
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t n = (uint64_t)dims.x * dims.y * dims.z;
-  if (i >= n)
-    return;
-  const uint32_t x = (uint32_t)(i % dims.x), y = (uint32_t)((i / dims.x) % dims.y),
-                 z = (uint32_t)(i / ((uint64_t)dims.x * dims.y));
-  dst[brickIndex(x, y, z, superX, superY)] = src[i];
-}
-
 }  // namespace
 
 void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint64_t *vox2,
@@ -402,33 +539,37 @@ void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint
   cudaCheck(cudaGetLastError(), "dense tree kernels");
 }
 
-void launchDenseLeafRanges(const DevGrid &g, uint32_t attr, const uint32_t nl[3],
-                           float *leafRanges, float *scratch, cudaStream_t st)
+void launchDenseBrickRanges(const void *src, uint32_t type, void *dst, const uint32_t dims[3],
+                            uint32_t superX, uint32_t superY, float background, float *leafRanges,
+                            cudaStream_t st)
 {
-  (void)scratch;
-  const uint3 NL      = {nl[0], nl[1], nl[2]};
-  const uint64_t n    = (uint64_t)nl[0] * nl[1] * nl[2];
-  const unsigned grid = blocksFor(n, 256);
-  switch (g.type[attr]) {
+  const uint3 D  = {dims[0], dims[1], dims[2]};
+  const uint3 NL = {(dims[0] + 7) / 8, (dims[1] + 7) / 8, (dims[2] + 7) / 8};
+  const dim3 grid((NL.x + 3) / 4, (NL.y + 3) / 4, (NL.z + kDenseChunk - 1) / kDenseChunk);
+#define VKL_DENSE_BRICK(T)                                                                              \
+  kDenseBrickRanges<T><<<grid, 256, 0, st>>>((const T *)src, (T *)dst, D, NL, superX, superY, background, \
+                                             leafRanges)
+  switch (type) {
   case kUChar:
-    kDenseLeafRanges<uint8_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(uint8_t);
     break;
   case kShort:
-    kDenseLeafRanges<int16_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(int16_t);
     break;
   case kUShort:
-    kDenseLeafRanges<uint16_t><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(uint16_t);
     break;
   case kHalf:
-    kDenseLeafRanges<__half><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(__half);
     break;
   case kDouble:
-    kDenseLeafRanges<double><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(double);
     break;
   default:
-    kDenseLeafRanges<float><<<grid, 256, 0, st>>>(g, attr, NL, leafRanges);
+    VKL_DENSE_BRICK(float);
   }
-  cudaCheck(cudaGetLastError(), "dense leaf range kernel");
+#undef VKL_DENSE_BRICK
+  cudaCheck(cudaGetLastError(), "dense bricking / leaf range kernel");
 }
 
 void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
@@ -502,28 +643,6 @@ void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves,
   else
     kCompressLeaves<<<grid, 256, 0, st>>>(src, numLeaves, 448.f, (__nv_fp8_storage_t *)codes, so);
   cudaCheck(cudaGetLastError(), "leaf compression kernel");
-}
-
-void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
-                     uint32_t superX, uint32_t superY, cudaStream_t st)
-{
-  const uint3 D = {dims[0], dims[1], dims[2]};
-  const uint64_t n = (uint64_t)dims[0] * dims[1] * dims[2];
-  const unsigned grid = blocksFor(n, 256);
-  switch (elemBytes) {
-  case 1:
-    kToBricked<uint8_t><<<grid, 256, 0, st>>>((const uint8_t *)src, (uint8_t *)dst, D, superX, superY);
-    break;
-  case 2:
-    kToBricked<uint16_t><<<grid, 256, 0, st>>>((const uint16_t *)src, (uint16_t *)dst, D, superX, superY);
-    break;
-  case 4:
-    kToBricked<uint32_t><<<grid, 256, 0, st>>>((const uint32_t *)src, (uint32_t *)dst, D, superX, superY);
-    break;
-  default:
-    kToBricked<uint64_t><<<grid, 256, 0, st>>>((const uint64_t *)src, (uint64_t *)dst, D, superX, superY);
-  }
-  cudaCheck(cudaGetLastError(), "bricking kernel");
 }
 
 }  // namespace vklcuda

@@ -11,7 +11,7 @@
 // function before it commits anything.  This entry point gives them the
 // commit path's range result (the filter-support window of every 8^3 leaf,
 // plus the background where a window leaves the volume; see
-// kDenseLeafRanges in k_build.cu) in one kernel launch on the device's stream,
+// kDenseBrickRanges in k_build.cu) in one kernel launch on the device's stream,
 // with its scratch in static device memory instead of an allocation.
 //
 // Scratch.  One file-scope __device__ array per device context, fixed size:
@@ -90,7 +90,7 @@ __device__ __forceinline__ void blockMinMax(float &lo, float &hi, float *slo, fl
 
 // One thread per leaf: the leaf's range over its window of the x-fastest
 // voxel array (same window and background rule as the commit path's
-// kDenseLeafRanges), reduced per block into the scratch partials; the block
+// kDenseBrickRanges), reduced per block into the scratch partials; the block
 // that finishes last reduces the partials into out[0..1] and re-arms the
 // counter.
 template <typename T>

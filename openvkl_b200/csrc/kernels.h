@@ -26,11 +26,9 @@ void launchBuildLeafMap(const DevGrid &g, uint64_t *map, cudaStream_t stream);
 // (scale, offset) float pair per leaf.
 void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,
                           float *scaleOffset, cudaStream_t stream);
-// Bricked copy of a dense x-fastest voxel array (brickIndex, grid.h):
-// returns the element count of the bricked array and its supertile counts.
+// Element count of the bricked copy of a dense x-fastest voxel array
+// (brickIndex, grid.h) and its supertile counts.
 uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY);
-void launchToBricked(const void *src, void *dst, size_t elemBytes, const uint32_t dims[3],
-                     uint32_t superX, uint32_t superY, cudaStream_t stream);
 
 // Commit-time tree construction for dense volumes: fills the voxel codes and
 // node origins of levels 0..2 (closed form of the reference's insertion
@@ -39,10 +37,13 @@ void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint
                           uint32_t *org1, uint32_t *org2, const uint32_t nl[3],
                           const uint32_t n1[3], const uint32_t n2[3], cudaStream_t stream);
 
-// Per-leaf value ranges (2 floats per leaf per attribute) of dense volumes:
-// min/max over each leaf's 3x3x3-leaf filter neighbourhood window.
-void launchDenseLeafRanges(const DevGrid &g, uint32_t attr, const uint32_t nl[3],
-                           float *leafRanges, float *scratch, cudaStream_t stream);
+// Dense commit of one attribute: writes the bricked copy of the x-fastest
+// voxel array `src` (element type `type`, kUChar..kDouble) to `dst`, and the
+// per-leaf value ranges (2 floats per leaf, leaves x-fastest) over each
+// leaf's 3x3x3-leaf filter neighbourhood window.
+void launchDenseBrickRanges(const void *src, uint32_t type, void *dst, const uint32_t dims[3],
+                            uint32_t superX, uint32_t superY, float background, float *leafRanges,
+                            cudaStream_t stream);
 // Same for sparse volumes, leaves given by root-relative offsets (3 u32).
 void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
                             const uint32_t *leafOffsets, float *leafRanges,

@@ -349,7 +349,16 @@ uint64_t packKey(uint32_t x, uint32_t y, uint32_t z)
 
 void Volume::commit()
 {
+  // Work that still reads the previous commit's buffers (on any stream)
+  // ends before they are reused, as it would before cudaFree.
+  if (!buffers.empty())
+    cudaCheck(cudaDeviceSynchronize(), "re-commit");
+  recycled = std::move(buffers);
   buffers.clear();
+  struct DropRecycled {
+    Volume *v;
+    ~DropRecycled() { v->recycled.clear(); }
+  } dropRecycled{this};
   keep.clear();
   committed = false;
   grid      = DevGrid{};
@@ -435,21 +444,6 @@ void Volume::commitDense()
     std::memcpy(c, cc, sizeof(c));
   }
   makeTransforms(c, grid.indexToObject, grid.objectToIndex);
-  // Each attribute is re-laid out once into the bricked order the kernels
-  // read (grid.h brickIndex); the padding of partial supertiles is zeroed
-  // and never read (every tap is checked against the domain first).
-  {
-    const uint32_t udims[3] = {(uint32_t)dims[0], (uint32_t)dims[1], (uint32_t)dims[2]};
-    const uint64_t nb = brickedElements(udims, grid.superX, grid.superY);
-    for (uint32_t a = 0; a < grid.numAttributes; ++a) {
-      const size_t es  = sizeOfType(attrs[a]->type);
-      DeviceBuffer *bb = newBuffer(nb * es);
-      cudaCheck(cudaMemsetAsync(bb->ptr, 0, nb * es, device->stream), "memset");
-      launchToBricked(attrs[a]->dev, bb->ptr, es, udims, grid.superX, grid.superY, device->stream);
-      grid.data[a] = bb->ptr;
-      grid.type[a] = attrs[a]->type;
-    }
-  }
   // background: one value, or one per attribute (ManagedObject.h:59-66)
   {
     std::vector<float> bg(grid.numAttributes, undefinedBackground());
@@ -504,11 +498,24 @@ void Volume::commitDense()
   launchBuildDenseTree(grid, v0->as<uint64_t>(), v1->as<uint64_t>(), v2->as<uint64_t>(),
                        o1->as<uint32_t>(), o2->as<uint32_t>(), nl, n1, n2, st);
 
-  DeviceBuffer leafRanges, volRange;
-  leafRanges.alloc(grid.numLeaves * 8);
-  volRange.alloc(8 * NA);
+  // Each attribute is re-laid out once into the bricked order the kernels
+  // read (grid.h brickIndex) by the same pass that computes its leaf ranges.
+  // The padding of partial supertiles is zeroed and never read (every tap is
+  // checked against the domain first).
+  // leaf ranges and the volume range: scratch of the commit, kept with the
+  // volume so that a re-commit reuses them
+  DeviceBuffer &leafRanges = *newBuffer(grid.numLeaves * 8), &volRange = *newBuffer(8 * NA);
+  const uint32_t udims[3] = {(uint32_t)dims[0], (uint32_t)dims[1], (uint32_t)dims[2]};
+  const uint64_t nb       = brickedElements(udims, grid.superX, grid.superY);
   for (uint32_t a = 0; a < grid.numAttributes; ++a) {
-    launchDenseLeafRanges(grid, a, nl, leafRanges.as<float>(), nullptr, st);
+    const size_t es  = sizeOfType(attrs[a]->type);
+    DeviceBuffer *bb = newBuffer(nb * es);
+    if (nb != nvox)
+      cudaCheck(cudaMemsetAsync(bb->ptr, 0, nb * es, st), "memset");
+    grid.data[a] = bb->ptr;
+    grid.type[a] = attrs[a]->type;
+    launchDenseBrickRanges(attrs[a]->dev, attrs[a]->type, bb->ptr, udims, grid.superX, grid.superY,
+                           grid.background[a], leafRanges.as<float>(), st);
     launchPropagateRanges(grid, a, grid.numLeaves, nullptr, leafRanges.as<float>(),
                           volRange.as<float>() + 2 * a, nl, st);
   }

@@ -258,8 +258,19 @@ struct Volume : ManagedObject {
 
   const char *typeName() const override { return isDense ? "structuredRegular" : "vdb"; }
   void commit() override;
+  // Device buffers of the previous commit.  A re-commit takes buffers of
+  // the sizes it needs from here (a time-varying volume re-committed with
+  // new data of the same shape allocates nothing); the rest are freed when
+  // the commit ends.
+  std::vector<std::unique_ptr<DeviceBuffer>> recycled;
   DeviceBuffer *newBuffer(size_t bytes)
   {
+    for (auto it = recycled.begin(); it != recycled.end(); ++it)
+      if ((*it)->bytes == bytes) {
+        buffers.push_back(std::move(*it));
+        recycled.erase(it);
+        return buffers.back().get();
+      }
     buffers.emplace_back(new DeviceBuffer());
     buffers.back()->alloc(bytes);
     return buffers.back().get();

@@ -109,6 +109,74 @@ def test_dense_tree_bit_exact(vkl, device, oracle):
     np.testing.assert_array_equal(vol.value_range(), ref.value_range())
 
 
+def _planted_field(dims, dtype, seed):
+    """A sinusoid field with NaN voxels, scattered -0.0 / +0.0 voxels, one
+    slab of mixed-sign zeros (whole leaf windows whose range is zero) and one
+    all-NaN block (leaf windows with no number at all)."""
+    X, Y, Z = dims
+    rng = np.random.default_rng(seed)
+    v = sinusoid_field(dims, seed=seed).astype(np.float64)
+    flat = v.reshape(-1)
+    n = flat.size
+    if np.issubdtype(dtype, np.floating):
+        flat[rng.choice(n, n // 200, replace=False)] = np.nan
+        flat[rng.choice(n, n // 200, replace=False)] = -0.0
+    flat[rng.choice(n, n // 200, replace=False)] = 0.0
+    v[Z // 3:Z // 3 + 12, :, :] = np.where(rng.random((min(12, Z - Z // 3), Y, X)) < 0.5, 0.0, -0.0)
+    if np.issubdtype(dtype, np.floating):
+        v[:10, :10, :10] = np.nan
+    if dtype == np.uint8:
+        return np.clip((v + 2.5) * 50, 0, 255).astype(np.uint8)
+    return v.astype(dtype)
+
+
+@pytest.mark.parametrize("dims", [(300, 140, 36), (77, 45, 19), (9, 8, 17)])
+@pytest.mark.parametrize("dtype", [np.float32, np.float16, np.float64, np.uint8])
+@pytest.mark.parametrize("background", [None, -2.0, -0.0, 0.0])
+def test_dense_leaf_ranges_nan_and_signed_zero(vkl, device, oracle, dims, dtype, background):
+    """Leaf ranges of dense volumes with NaN and -0.0 voxels: a NaN voxel
+    resets the running bound of the reference's fold (VdbSampler_dense.ih:
+    35-105), and a zero bound takes the sign of the zero the fold meets
+    last, so these windows depend on the fold order.  Compared bit for bit
+    on the leaves' parent level (one leaf per voxel).  Upper levels and the
+    volume range are compared by value: where +0.0 and -0.0 bounds of
+    different leaves tie, the sign follows the tie rule of rkcommon's
+    range1f::extend, which is not part of the reference tree."""
+    vox = _planted_field(dims, dtype, seed=11)
+    bg = None if background is None else [background]
+    ref = oracle.OracleVolume.dense_volume(vox, background=bg)
+    vol = vkl.structured_regular(device, vox, background=bg)
+    for level in range(3):
+        _, rng, org = vol.tree_level(level)
+        _, rrng, rorg = ref.level(level, 1)
+        np.testing.assert_array_equal(org, rorg)
+        if level == 2:
+            np.testing.assert_array_equal(bits(rng), bits(rrng))
+        else:
+            np.testing.assert_array_equal(rng, rrng)
+    np.testing.assert_array_equal(vol.value_range(), ref.value_range())
+    # the planted cases reach the reference-order path: some leaf ranges
+    # differ from the NaN-ignoring min / max of their windows
+    if np.issubdtype(dtype, np.floating) and background is None and dims[0] == 300:
+        X, Y, Z = dims
+        f = vox.astype(np.float32)
+        vox2, rng, _ = vol.tree_level(2)
+        leaf = (vox2 & 3) == 3
+        got = rng[leaf]
+        plain = []
+        for lz in range((Z + 7) // 8):
+            for ly in range((Y + 7) // 8):
+                for lx in range((X + 7) // 8):
+                    w = f[max(8 * lz - 1, 0):8 * lz + 10, max(8 * ly - 1, 0):8 * ly + 10,
+                          max(8 * lx - 1, 0):8 * lx + 10]
+                    w = w[~np.isnan(w)]
+                    plain.append((w.min(), w.max()) if w.size else (np.inf, -np.inf))
+        # leaves are x-fastest, level-2 voxels z-fastest within a node
+        plain = np.array(plain, np.float32)
+        assert len(plain) == len(got)
+        assert not np.array_equal(np.sort(bits(plain[:, 0])), np.sort(bits(got[:, 0])))
+
+
 def test_inner_node_observer_matches_oracle(vkl, device, oracle):
     origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=4)
     ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
