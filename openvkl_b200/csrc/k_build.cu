@@ -179,94 +179,128 @@ __device__ float2 denseLeafRangeExact(const T *__restrict__ src, uint3 dims, int
   return make_float2(lo, hi);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) kDenseBrickRanges(const T *__restrict__ src, T *__restrict__ dst,
-                                                         uint3 dims, uint3 nl, uint32_t superX, uint32_t superY,
-                                                         float bg, float *__restrict__ leafRanges)
+// Per-plane steps shared by both kernels.  `at(r, c)` is the voxel at
+// (x, y) = (X0 - 1 + c, Y0 - 1 + r) of the staged 35x35 window.
+struct TileCoords {
+  int32_t X0, Y0, X, Y, Z;
+  int32_t k0, k1, zBeg, zEnd;
+};
+
+__device__ __forceinline__ TileCoords tileCoords(uint3 dims, uint3 nl)
 {
-  __shared__ T plane[kPlaneW][kPlaneW];
-  __shared__ PartialRange xres[kPlaneW][4];
-  __shared__ PartialRange pres[kMaxPlanes][16];
-  const int tid   = threadIdx.x;
-  const int32_t X0 = 32 * (int32_t)blockIdx.x, Y0 = 32 * (int32_t)blockIdx.y;
-  const int32_t X = (int32_t)dims.x, Y = (int32_t)dims.y, Z = (int32_t)dims.z;
-  const int32_t k0 = kDenseChunk * (int32_t)blockIdx.z, k1 = min(k0 + kDenseChunk, (int32_t)nl.z);
-  const int32_t zBeg = max(8 * k0 - 1, 0), zEnd = min(8 * k1 + 2, Z);
-  // The next plane is loaded into registers while the current one is
-  // reduced, so the loads of one plane overlap the work on the previous.
-  constexpr int kPerThread = (kPlaneW * kPlaneW + 255) / 256;
-  T next[kPerThread];
-  auto loadPlane = [&](int32_t z) {
-    const uint64_t zoff = (uint64_t)z * dims.y;
+  TileCoords t;
+  t.X0 = 32 * (int32_t)blockIdx.x;
+  t.Y0 = 32 * (int32_t)blockIdx.y;
+  t.X = (int32_t)dims.x, t.Y = (int32_t)dims.y, t.Z = (int32_t)dims.z;
+  t.k0   = kDenseChunk * (int32_t)blockIdx.z;
+  t.k1   = min(t.k0 + kDenseChunk, (int32_t)nl.z);
+  t.zBeg = max(8 * t.k0 - 1, 0);
+  t.zEnd = min(8 * t.k1 + 2, t.Z);
+  return t;
+}
+
+// A thread's part of the bricked copy of a plane's 32x32 interior: column
+// x = X0 + (tid & 31), rows y = Y0 + (tid >> 5) + 8u.  brickIndex is a sum
+// of per-axis terms, so the x and y terms are computed once per thread and
+// the z term once per plane.
+struct BrickWriter {
+  uint64_t termXY[4];
+  uint32_t valid;  // bit u: (x, y_u) inside the volume
+  uint64_t zStride;
+
+  __device__ __forceinline__ BrickWriter(const TileCoords &t, uint32_t superX, uint32_t superY)
+  {
+    const uint32_t x = (uint32_t)(t.X0 + (threadIdx.x & 31));
+    const uint64_t tx = ((uint64_t)(x >> 6) << 18) + (((x >> 3) & 7u) << 9) + (x & 7u);
+    const uint64_t yStride = (uint64_t)superX << 18;
+    zStride = (uint64_t)superX * superY << 18;
+    valid   = 0;
 #pragma unroll
-    for (int u = 0; u < kPerThread; ++u) {
-      const int e = tid + 256 * u, r = e / kPlaneW, c = e - r * kPlaneW;
-      const int32_t y = Y0 - 1 + r, x = X0 - 1 + c;
-      if (e < kPlaneW * kPlaneW && (uint32_t)x < dims.x && (uint32_t)y < dims.y)
-        next[u] = src[(zoff + y) * dims.x + x];
-    }
-  };
-  loadPlane(zBeg);
-  for (int32_t z = zBeg; z < zEnd; ++z) {
-#pragma unroll
-    for (int u = 0; u < kPerThread; ++u) {
-      const int e = tid + 256 * u;
-      if (e < kPlaneW * kPlaneW)
-        plane[e / kPlaneW][e % kPlaneW] = next[u];
-    }
-    __syncthreads();
-    if (z + 1 < zEnd)
-      loadPlane(z + 1);
-    if (z >= 8 * k0 && z < 8 * k1) {
-      for (int e = tid; e < 1024; e += 256) {
-        const int32_t y = Y0 + (e >> 5), x = X0 + (e & 31);
-        if (x < X && y < Y)
-          dst[brickIndex((uint32_t)x, (uint32_t)y, (uint32_t)z, superX, superY)] = plane[(e >> 5) + 1][(e & 31) + 1];
-      }
-    }
-    if (tid < kPlaneW * 4) {
-      const int r = tid >> 2, i = tid & 3;
-      const int32_t y = Y0 - 1 + r;
-      PartialRange pr{kInf, -kInf, 0u};
-      if ((uint32_t)y < dims.y && X0 + 8 * i < X) {
-        const int c0 = max(8 * i, 1 - X0), c1 = min(8 * i + 11, X - X0 + 1);
-        for (int c = c0; c < c1; ++c) {
-          const float v = toFloat(plane[r][c]);
-          pr.flag |= orderFlags(v);
-          pr.lo = fminf(pr.lo, v);
-          pr.hi = fmaxf(pr.hi, v);
-        }
-      }
-      xres[r][i] = pr;
-    }
-    __syncthreads();
-    if (tid < 16) {
-      const int i = tid & 3, j = tid >> 2;
-      PartialRange pr{kInf, -kInf, 0u};
-      for (int r = 8 * j; r < 8 * j + 11; ++r) {
-        const PartialRange q = xres[r][i];
-        pr.lo = fminf(pr.lo, q.lo);
-        pr.hi = fmaxf(pr.hi, q.hi);
-        pr.flag |= q.flag;
-      }
-      pres[z - zBeg][tid] = pr;
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t y = (uint32_t)(t.Y0 + (threadIdx.x >> 5) + 8 * u);
+      termXY[u] = tx + (uint64_t)(y >> 6) * yStride + ((((y >> 3) & 7u) << 12) + ((y & 7u) << 3));
+      if ((int32_t)x < t.X && (int32_t)y < t.Y)
+        valid |= 1u << u;
     }
   }
-  __syncthreads();
+  template <typename T, class At>
+  __device__ __forceinline__ void write(uint32_t z, At at, T *__restrict__ dst) const
+  {
+    const uint64_t tz = (uint64_t)(z >> 6) * zStride + ((((z >> 3) & 7u) << 15) + ((z & 7u) << 6));
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (valid & (1u << u))
+        dst[termXY[u] + tz] = at((threadIdx.x >> 5) + 8 * u + 1, (threadIdx.x & 31) + 1);
+  }
+};
+
+// Bricked copy of the plane's interior and the per-row ranges of the four
+// leaf x-windows (into xres).
+template <typename T, class At>
+__device__ __forceinline__ void planeRows(const TileCoords &t, int32_t z, At at, T *__restrict__ dst,
+                                          const BrickWriter &bw, PartialRange (*xres)[4])
+{
+  const int tid = threadIdx.x;
+  if (z >= 8 * t.k0 && z < 8 * t.k1)
+    bw.write((uint32_t)z, at, dst);
+  if (tid < kPlaneW * 4) {
+    const int r = tid >> 2, i = tid & 3;
+    const int32_t y = t.Y0 - 1 + r;
+    PartialRange pr{kInf, -kInf, 0u};
+    auto fold = [&](int c) {
+      const float v = toFloat(at(r, c));
+      pr.flag |= orderFlags(v);
+      pr.lo = fminf(pr.lo, v);
+      pr.hi = fmaxf(pr.hi, v);
+    };
+    if ((uint32_t)y < (uint32_t)t.Y && t.X0 + 8 * i < t.X) {
+      const int c0 = max(8 * i, 1 - t.X0), c1 = min(8 * i + 11, t.X - t.X0 + 1);
+      for (int c = c0; c < c1; ++c)
+        fold(c);
+    }
+    xres[r][i] = pr;
+  }
+}
+
+// The plane's range per leaf column (threads 0..15).
+__device__ __forceinline__ void planeColumns(const PartialRange (*xres)[4], PartialRange *out)
+{
+  const int tid = threadIdx.x;
+  if (tid < 16) {
+    const int i = tid & 3, j = tid >> 2;
+    PartialRange pr{kInf, -kInf, 0u};
+    for (int r = 8 * j; r < 8 * j + 11; ++r) {
+      const PartialRange q = xres[r][i];
+      pr.lo = fminf(pr.lo, q.lo);
+      pr.hi = fmaxf(pr.hi, q.hi);
+      pr.flag |= q.flag;
+    }
+    out[tid] = pr;
+  }
+}
+
+// Folds 11 plane ranges per leaf and writes the leaf ranges (one thread per
+// leaf of the CTA's column).
+template <typename T>
+__device__ __forceinline__ void finishLeaves(const TileCoords &t, const PartialRange (*pres)[16],
+                                             const T *__restrict__ src, uint3 dims, uint3 nl, float bg,
+                                             float *__restrict__ leafRanges)
+{
+  const int tid = threadIdx.x;
   const int layer = tid >> 4, col = tid & 15;
   const int32_t lx = 4 * (int32_t)blockIdx.x + (col & 3), ly = 4 * (int32_t)blockIdx.y + (col >> 2),
-                lz = k0 + layer;
-  if (layer >= kDenseChunk || lz >= k1 || lx >= (int32_t)nl.x || ly >= (int32_t)nl.y)
+                lz = t.k0 + layer;
+  if (layer >= kDenseChunk || lz >= t.k1 || lx >= (int32_t)nl.x || ly >= (int32_t)nl.y)
     return;
   PartialRange pr{kInf, -kInf, 0u};
-  for (int32_t z = max(8 * lz - 1, 0); z < min(8 * lz + 10, Z); ++z) {
-    const PartialRange q = pres[z - zBeg][col];
+  for (int32_t z = max(8 * lz - 1, 0); z < min(8 * lz + 10, t.Z); ++z) {
+    const PartialRange q = pres[z - t.zBeg][col];
     pr.lo = fminf(pr.lo, q.lo);
     pr.hi = fmaxf(pr.hi, q.hi);
     pr.flag |= q.flag;
   }
   const int32_t ox = 8 * lx, oy = 8 * ly, oz = 8 * lz;
-  const bool boundary = lx == 0 || ly == 0 || lz == 0 || ox + 8 >= X || oy + 8 >= Y || oz + 8 >= Z;
+  const bool boundary = lx == 0 || ly == 0 || lz == 0 || ox + 8 >= t.X || oy + 8 >= t.Y || oz + 8 >= t.Z;
   float2 r = make_float2(pr.lo, pr.hi);
   if (boundary && !isnan(bg)) {
     r.x = fminf(r.x, bg);
@@ -278,6 +312,61 @@ __global__ void __launch_bounds__(256) kDenseBrickRanges(const T *__restrict__ s
   const uint64_t leaf = ((uint64_t)lz * nl.y + ly) * nl.x + lx;
   leafRanges[2 * leaf]     = r.x;
   leafRanges[2 * leaf + 1] = r.y;
+}
+
+// Any row pitch: the next plane is loaded into registers while the current
+// one is reduced.
+template <typename T>
+__global__ void __launch_bounds__(256, 4) kDenseBrickRanges(const T *__restrict__ src, T *__restrict__ dst,
+                                                         uint3 dims, uint3 nl, uint32_t superX, uint32_t superY,
+                                                         float bg, float *__restrict__ leafRanges)
+{
+  __shared__ T plane[kPlaneW][kPlaneW];
+  __shared__ PartialRange xres[kPlaneW][4];
+  __shared__ PartialRange pres[kMaxPlanes][16];
+  const int tid        = threadIdx.x;
+  const TileCoords t   = tileCoords(dims, nl);
+  const BrickWriter bw(t, superX, superY);
+  // Loads: 245 threads = 7 rows x 35 columns per pass, 5 passes cover the
+  // 35 rows.  A thread's column and its row validity are fixed; its voxel
+  // offset within a plane is rowOff + 7 * u * X.
+  constexpr int kRowsPerPass = 7, kPasses = kPlaneW / kRowsPerPass;
+  const int lr = tid / kPlaneW, lc = tid - lr * kPlaneW;
+  const bool loader = tid < kRowsPerPass * kPlaneW;
+  const int32_t lx = t.X0 - 1 + lc;
+  uint32_t rowValid = 0;
+#pragma unroll
+  for (int u = 0; u < kPasses; ++u)
+    if (loader && (uint32_t)lx < dims.x && (uint32_t)(t.Y0 - 1 + lr + kRowsPerPass * u) < dims.y)
+      rowValid |= 1u << u;
+  // the first row may lie above the volume (then only the later passes load)
+  const int64_t rowOff     = (int64_t)(t.Y0 - 1 + lr) * dims.x + lx;
+  const int64_t planeElems = (int64_t)dims.x * dims.y, passStride = (int64_t)kRowsPerPass * dims.x;
+  T next[kPasses];
+  auto loadPlane = [&](int32_t z) {
+    const T *p = src + ((int64_t)z * planeElems + rowOff);
+#pragma unroll
+    for (int u = 0; u < kPasses; ++u)
+      if (rowValid & (1u << u))
+        next[u] = p[u * passStride];
+  };
+  auto at = [&](int r, int c) { return plane[r][c]; };
+  loadPlane(t.zBeg);
+  for (int32_t z = t.zBeg; z < t.zEnd; ++z) {
+    if (loader) {
+#pragma unroll
+      for (int u = 0; u < kPasses; ++u)
+        plane[lr + kRowsPerPass * u][lc] = next[u];
+    }
+    __syncthreads();
+    if (z + 1 < t.zEnd)
+      loadPlane(z + 1);
+    planeRows(t, z, at, dst, bw, xres);
+    __syncthreads();
+    planeColumns(xres, pres[z - t.zBeg]);
+  }
+  __syncthreads();
+  finishLeaves(t, pres, src, dims, nl, bg, leafRanges);
 }
 
 // ---------------------------------------------------------------------------

@@ -130,7 +130,7 @@ def _planted_field(dims, dtype, seed):
     return v.astype(dtype)
 
 
-@pytest.mark.parametrize("dims", [(300, 140, 36), (77, 45, 19), (9, 8, 17)])
+@pytest.mark.parametrize("dims", [(300, 140, 36), (320, 40, 24), (77, 45, 19), (9, 8, 17)])
 @pytest.mark.parametrize("dtype", [np.float32, np.float16, np.float64, np.uint8])
 @pytest.mark.parametrize("background", [None, -2.0, -0.0, 0.0])
 def test_dense_leaf_ranges_nan_and_signed_zero(vkl, device, oracle, dims, dtype, background):
