@@ -366,8 +366,14 @@ void Volume::commit()
   gradientFilter = getInt("gradientFilter", filter);
   maxSamplingDepth = (uint32_t)std::min(getInt("maxSamplingDepth", (int)kNumLevels - 1),
                                         (int)kNumLevels - 1);
-  if (has("temporallyStructuredNumTimesteps") || has("temporallyUnstructuredIndices") ||
-      has("node.temporallyStructuredNumTimesteps") || has("node.temporallyUnstructuredIndices"))
+  // Temporal parameters describing temporally constant data are accepted,
+  // as the reference accepts them: a structuredRegular volume is temporally
+  // varying only with temporallyStructuredNumTimesteps > 0 or a
+  // temporallyUnstructuredIndices array (DenseVdbVolume.cpp:149-186), a vdb
+  // node only with a non-constant node.temporalFormat (checked in
+  // commitVdb).  The reference's VdbVolumeBuffers utility sets the node.*
+  // temporal arrays on every volume it creates.
+  if (isDense && (getInt("temporallyStructuredNumTimesteps", 0) > 0 || getData("temporallyUnstructuredIndices")))
     fail("temporally varying (motion blur) volumes are not supported by the cuda device",
          VKL_INVALID_OPERATION);
   if (isDense)
@@ -551,11 +557,22 @@ void Volume::commitVdb()
     fail("node.level, node.origin, node.format, node.temporalFormat, and node.data must all have "
          "the same size");
   if (Data *tf = getData("node.temporalFormat")) {
+    if (tf->numItems != numLeaves)
+      fail("node.level, node.origin, node.format, node.temporalFormat, and node.data must all have "
+           "the same size");
     const uint32_t *t = tf->hostAs<uint32_t>();
     for (uint64_t i = 0; i < tf->numItems; ++i)
       if (t[i] != 0)
         fail("temporally varying (motion blur) volumes are not supported by the cuda device",
              VKL_INVALID_OPERATION);
+  }
+  // present with constant nodes: size-checked as the reference does
+  // (VdbVolume.cpp:720-746), otherwise unused
+  for (const char *name : {"node.temporallyStructuredNumTimesteps", "node.temporallyUnstructuredIndices",
+                           "node.temporallyUnstructuredTimes"}) {
+    Data *d = getData(name);
+    if (d && d->numItems != numLeaves)
+      fail(std::string("If ") + name + " is set, it must have the same size as node.data");
   }
   const uint32_t *levels = dLevel->hostAs<uint32_t>();
   const int32_t *origins = dOrigin->hostAs<int32_t>();

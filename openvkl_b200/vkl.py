@@ -357,11 +357,13 @@ class Data(_Obj):
                  shared: bool = False, objects: Optional[Sequence["Data"]] = None,
                  num_items: Optional[int] = None, byte_stride: int = 0):
         if objects is not None:
-            arr = (VKLObject * len(objects))(*[o.h for o in objects])
+            # None entries become null handles (e.g. the per-node temporal
+            # arrays of temporally constant vdb nodes)
+            arr = (VKLObject * len(objects))(*[o.h if o is not None else VKLObject() for o in objects])
             h = device.lib.vklNewData(device.handle, len(objects), VKL_DATA, C.cast(arr, C.c_void_p),
                                       VKL_DATA_DEFAULT, 0)
             super().__init__(device, h)
-            self._keep = list(objects)
+            self._keep = [o for o in objects if o is not None]
             self._check_handle("vklNewData")
             return
         if _is_torch(array):

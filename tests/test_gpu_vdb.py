@@ -197,6 +197,81 @@ def test_vdb_validation_errors(vkl, device):
         vkl.vdb_volume(device, [3], [[0, 0, 0]], [1], node_data=[data[:1]])
 
 
+def _volume_buffers_style(vkl, device, levels, origins, formats, node_data, temporal_format=None,
+                          structured_steps=None):
+    """A vdb volume with the parameter set the reference's VdbVolumeBuffers
+    utility gives every volume it creates (utility/vdb/include/openvkl/
+    utility/vdb/VdbVolumeBuffers.h:668-816): node.temporalFormat, the
+    per-node temporal arrays (zeros / null data handles for constant nodes),
+    indexToObject, and node.data."""
+    n = len(levels)
+    v = vkl.Volume(device, "vdb")
+    v.set_param("indexToObject", vkl.VKL_AFFINE3F, np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32))
+    v.set_data("node.level", vkl.Data(device, np.ascontiguousarray(levels, np.uint32)))
+    v.set_data("node.origin", vkl.Data(device, np.ascontiguousarray(origins, np.int32).reshape(-1),
+                                       vkl_type=vkl.VKL_VEC3I))
+    v.set_data("node.format", vkl.Data(device, np.ascontiguousarray(formats, np.uint32)))
+    tf = np.zeros(n, np.uint32) if temporal_format is None else temporal_format
+    v.set_data("node.temporalFormat", vkl.Data(device, tf))
+    steps = np.zeros(n, np.int32) if structured_steps is None else structured_steps
+    v.set_data("node.temporallyStructuredNumTimesteps", vkl.Data(device, steps))
+    v.set_data("node.temporallyUnstructuredIndices", vkl.Data(device, objects=[None] * n))
+    v.set_data("node.temporallyUnstructuredTimes", vkl.Data(device, objects=[None] * n))
+    v.set_data("node.data", vkl.Data(device, objects=[vkl.Data(device, a) for a in node_data]))
+    v.commit()
+    return v
+
+
+def test_vdb_volume_buffers_parameter_set(vkl, device, oracle):
+    """Volumes made by the reference's VdbVolumeBuffers (the path OpenVDB
+    ingestion takes) carry temporal parameters even when every node is
+    temporally constant; they commit and sample like volumes without them.
+    A non-constant node and mis-sized temporal arrays are rejected."""
+    origins, levels, formats, vals, tvals = _shell_vdb(domain=64, seed=3)
+    n_dense = len(vals) // 512
+    node_data = [vals[i * 512:(i + 1) * 512] for i in range(n_dense)] + [tvals[i:i + 1] for i in range(len(tvals))]
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tvals)
+    vol = _volume_buffers_style(vkl, device, levels, origins, formats, node_data)
+    plain = vkl.vdb_volume(device, levels, origins, formats, node_data=node_data)
+    # node.data input: leaf pointers hold node indices (VdbVolume.cpp:306-317),
+    # so the tree is compared with the same input minus the temporal arrays
+    for level in range(3):
+        for a, b in zip(vol.tree_level(level), plain.tree_level(level)):
+            np.testing.assert_array_equal(a, b)
+    rng = np.random.default_rng(8)
+    pts = (origins[rng.integers(0, len(origins), 8000)] + rng.uniform(-1, 9, (8000, 3))).astype(np.float32)
+    for fv in (0, 100, 200):
+        got = vkl.Sampler(vol, filter=fv).sample(pts)
+        np.testing.assert_array_equal(bits(got), bits(vkl.Sampler(plain, filter=fv).sample(pts)))
+        np.testing.assert_array_equal(bits(got), bits(ref.sample(pts, filter=fv)))
+    n = len(levels)
+    moving = np.zeros(n, np.uint32)
+    moving[0] = 1  # VKL_TEMPORAL_FORMAT_STRUCTURED
+    with pytest.raises(vkl.VKLError, match="temporally varying"):
+        _volume_buffers_style(vkl, device, levels, origins, formats, node_data, temporal_format=moving)
+    with pytest.raises(vkl.VKLError, match="If node.temporallyStructuredNumTimesteps is set, it must have the "
+                                           "same size as node.data"):
+        _volume_buffers_style(vkl, device, levels, origins, formats, node_data,
+                              structured_steps=np.zeros(n - 1, np.int32))
+
+
+def test_dense_temporal_parameters(vkl, device, oracle):
+    """structuredRegular: temporallyStructuredNumTimesteps = 0 means constant
+    data (DenseVdbVolume.cpp:149-186) and is accepted; > 0 is rejected."""
+    vox = sinusoid_field((20, 18, 16), seed=2)
+    v = vkl.Volume(device, "structuredRegular")
+    v.set_vec3i("dimensions", (20, 18, 16))
+    v.set_int("temporallyStructuredNumTimesteps", 0)
+    v.set_data("data", vkl.Data(device, vox))
+    v.commit()
+    ref = oracle.OracleVolume.dense_volume(vox)
+    pts = uniform_points(4000, (0, 0, 0), (19, 17, 15), seed=5)
+    np.testing.assert_array_equal(bits(vkl.Sampler(v).sample(pts)), bits(ref.sample(pts)))
+    v.set_int("temporallyStructuredNumTimesteps", 2)
+    with pytest.raises(vkl.VKLError, match="temporally varying"):
+        v.commit()
+
+
 @pytest.mark.parametrize("fv,depth", [(0, 3), (100, 3), (200, 3), (100, 1)])
 def test_leaf_access_observer(vkl, device, oracle, fv, depth):
     """vklNewSamplerObserver(sampler, "LeafNodeAccess"): after sampling, the
