@@ -15,8 +15,10 @@
 // device's CUDA stream (vklDeviceSetVoidPtr(device, "cudaStream", stream)).
 #pragma once
 
+#include <stdbool.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>  // as the reference's sampler.h / volume.h / observer.h
 
 #ifdef __cplusplus
 extern "C" {
@@ -187,6 +189,32 @@ OPENVKL_CUDA_INTERFACE void vklComputeSample16(const int *valid, const VKLSample
                                                const vkl_vvec3f16 *objectCoordinates,
                                                float *samples, unsigned int attributeIndex,
                                                const float *times);
+// Multi-attribute samples of 4 / 8 / 16 SoA points; samples[m * W + i] is
+// attribute attributeIndices[m] at lane i (openvkl/devices/cpu/include/
+// openvkl/device/openvkl.h:79-104).
+OPENVKL_CUDA_INTERFACE void vklComputeSampleM4(const int *valid, const VKLSampler *sampler,
+                                               const vkl_vvec3f4 *objectCoordinates, float *samples,
+                                               unsigned int M, const unsigned int *attributeIndices,
+                                               const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSampleM8(const int *valid, const VKLSampler *sampler,
+                                               const vkl_vvec3f8 *objectCoordinates, float *samples,
+                                               unsigned int M, const unsigned int *attributeIndices,
+                                               const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeSampleM16(const int *valid, const VKLSampler *sampler,
+                                                const vkl_vvec3f16 *objectCoordinates, float *samples,
+                                                unsigned int M, const unsigned int *attributeIndices,
+                                                const float *times);
+// Gradients of 4 / 8 / 16 SoA points (openvkl/devices/cpu/include/openvkl/
+// device/openvkl.h:121-143).
+OPENVKL_CUDA_INTERFACE void vklComputeGradient4(const int *valid, const VKLSampler *sampler,
+                                                const vkl_vvec3f4 *objectCoordinates, vkl_vvec3f4 *gradients,
+                                                unsigned int attributeIndex, const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeGradient8(const int *valid, const VKLSampler *sampler,
+                                                const vkl_vvec3f8 *objectCoordinates, vkl_vvec3f8 *gradients,
+                                                unsigned int attributeIndex, const float *times);
+OPENVKL_CUDA_INTERFACE void vklComputeGradient16(const int *valid, const VKLSampler *sampler,
+                                                 const vkl_vvec3f16 *objectCoordinates, vkl_vvec3f16 *gradients,
+                                                 unsigned int attributeIndex, const float *times);
 OPENVKL_CUDA_INTERFACE void vklComputeSampleN(const VKLSampler *sampler,
                                               unsigned int N,
                                               const vkl_vec3f *objectCoordinates,

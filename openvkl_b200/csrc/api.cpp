@@ -258,8 +258,8 @@ void sampleW(const int *valid, const VKLSampler *sampler, const V *oc, float *sa
       pts[n] = {oc->x[i], oc->y[i], oc->z[i]};
       idx[n++] = i;
     }
-  float out[W * kMaxAttributes];
-  sampleN(sampler, (uint64_t)n, pts, out, M, attrs);
+  std::vector<float> out((size_t)W * M);
+  sampleN(sampler, (uint64_t)n, pts, out.data(), M, attrs);
   for (int k = 0; k < n; ++k)
     for (uint32_t m = 0; m < M; ++m)
       samples[m * W + idx[k]] = out[k * M + m];
@@ -669,6 +669,38 @@ void vklComputeSample16(const int *valid, const VKLSampler *s, const vkl_vvec3f1
 {
   guardedVoid(s ? deviceOf(*s) : g_lastDevice,
               [&]() { sampleW<16>(valid, s, oc, samples, 1, &attr); });
+}
+
+void vklComputeSampleM4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc, float *samples,
+                        unsigned int M, const unsigned int *attrs, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<4>(valid, s, oc, samples, M, attrs); });
+}
+void vklComputeSampleM8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc, float *samples,
+                        unsigned int M, const unsigned int *attrs, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<8>(valid, s, oc, samples, M, attrs); });
+}
+void vklComputeSampleM16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc, float *samples,
+                         unsigned int M, const unsigned int *attrs, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<16>(valid, s, oc, samples, M, attrs); });
+}
+
+void vklComputeGradient4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc, vkl_vvec3f4 *grads,
+                         unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<4>(valid, s, oc, grads, attr); });
+}
+void vklComputeGradient8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc, vkl_vvec3f8 *grads,
+                         unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<8>(valid, s, oc, grads, attr); });
+}
+void vklComputeGradient16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc,
+                          vkl_vvec3f16 *grads, unsigned int attr, const float *)
+{
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<16>(valid, s, oc, grads, attr); });
 }
 
 void vklComputeSampleN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,

@@ -58,6 +58,8 @@ EXPORTS = [
     "vklSetParam", "vklNewSampler", "vklGetFeatureFlags", "vklComputeSample",
     "vklComputeSample4", "vklComputeSample8", "vklComputeSample16", "vklComputeSampleN",
     "vklComputeSampleM", "vklComputeSampleMN", "vklComputeGradient", "vklComputeGradientN",
+    "vklComputeSampleM4", "vklComputeSampleM8", "vklComputeSampleM16",
+    "vklComputeGradient4", "vklComputeGradient8", "vklComputeGradient16",
     "vklNewIntervalIteratorContext", "vklNewHitIteratorContext", "vklGetIntervalIteratorSize",
     "vklInitIntervalIterator", "vklIterateInterval", "vklGetHitIteratorSize",
     "vklInitHitIterator", "vklIterateHit", "vklIterateIntervalsN", "vklIterateHitsN",
@@ -173,6 +175,12 @@ def load_library(path: str = LIB_PATH, load_only: bool = False) -> C.CDLL:
         "vklComputeSampleMN": (None, [C.POINTER(O), U, VP, VP, U, VP, VP]),
         "vklComputeGradient": (vec3f, [C.POINTER(O), C.POINTER(vec3f), U, F]),
         "vklComputeGradientN": (None, [C.POINTER(O), U, VP, VP, U, VP]),
+        "vklComputeSampleM4": (None, [VP, C.POINTER(O), C.POINTER(vvec3f4), VP, U, VP, VP]),
+        "vklComputeSampleM8": (None, [VP, C.POINTER(O), C.POINTER(vvec3f8), VP, U, VP, VP]),
+        "vklComputeSampleM16": (None, [VP, C.POINTER(O), C.POINTER(vvec3f16), VP, U, VP, VP]),
+        "vklComputeGradient4": (None, [VP, C.POINTER(O), C.POINTER(vvec3f4), C.POINTER(vvec3f4), U, VP]),
+        "vklComputeGradient8": (None, [VP, C.POINTER(O), C.POINTER(vvec3f8), C.POINTER(vvec3f8), U, VP]),
+        "vklComputeGradient16": (None, [VP, C.POINTER(O), C.POINTER(vvec3f16), C.POINTER(vvec3f16), U, VP]),
         "vklNewIntervalIteratorContext": (O, [O]),
         "vklNewHitIteratorContext": (O, [O]),
         "vklGetIntervalIteratorSize": (SZ, [C.POINTER(O)]),
@@ -733,6 +741,36 @@ class Sampler(_Obj):
         out = np.full(W, np.nan, np.float32)
         self._call(fn, vmask.ctypes.data, C.byref(self.h), C.byref(soa), out.ctypes.data, attr, None)
         return out
+
+    @staticmethod
+    def _soa(points):
+        T = {4: vvec3f4, 8: vvec3f8, 16: vvec3f16}[len(points)]
+        soa = T()
+        for i, p in enumerate(points):
+            soa.x[i], soa.y[i], soa.z[i] = (float(p[0]), float(p[1]), float(p[2]))
+        return soa
+
+    def sample_m_w(self, points, attrs, valid=None):
+        """vklComputeSampleM4/8/16: (M, W) samples, row m = attribute attrs[m]."""
+        W = len(points)
+        fn = {4: self.lib.vklComputeSampleM4, 8: self.lib.vklComputeSampleM8, 16: self.lib.vklComputeSampleM16}[W]
+        a = np.ascontiguousarray(attrs, np.uint32)
+        vmask = np.ones(W, np.int32) if valid is None else np.asarray(valid, np.int32)
+        out = np.full((len(a), W), np.nan, np.float32)
+        self._call(fn, vmask.ctypes.data, C.byref(self.h), C.byref(self._soa(points)), out.ctypes.data, len(a),
+                   a.ctypes.data, None)
+        return out
+
+    def gradient_w(self, points, valid=None, attr=0):
+        """vklComputeGradient4/8/16: (W, 3) gradients (invalid lanes NaN)."""
+        W = len(points)
+        fn = {4: self.lib.vklComputeGradient4, 8: self.lib.vklComputeGradient8,
+              16: self.lib.vklComputeGradient16}[W]
+        vmask = np.ones(W, np.int32) if valid is None else np.asarray(valid, np.int32)
+        g = self._soa(np.full((W, 3), np.nan))
+        self._call(fn, vmask.ctypes.data, C.byref(self.h), C.byref(self._soa(points)), C.byref(g), attr, None)
+        return np.stack([np.array(g.x[:], np.float32), np.array(g.y[:], np.float32),
+                         np.array(g.z[:], np.float32)], 1)
 
 
 class IntervalIteratorContext(_Obj):

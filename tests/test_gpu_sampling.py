@@ -118,6 +118,29 @@ def test_scalar_and_wide_entry_points(vkl, device, oracle):
         valid = (np.arange(w) % 3 != 1).astype(np.int32)
         got = smp.sample_w(pts[:w], valid=valid)
         np.testing.assert_array_equal(bits(got[valid == 1]), bits(want[:w][valid == 1]))
+        g = smp.gradient_w(pts[:w], valid=valid)
+        gw = ref.gradient(pts[:w], filter=200)
+        np.testing.assert_array_equal(bits(g[valid == 1]), bits(gw[valid == 1]))
+        assert np.isnan(g[valid == 0]).all()  # invalid lanes are not written
+
+
+def test_wide_multi_attribute_entry_points(vkl, device, oracle):
+    """vklComputeSampleM4/8/16: samples[m * W + lane] is attribute
+    attributeIndices[m] at that lane (the layout the reference tutorial
+    prints, examples/vklTutorialCPU.c:212-231)."""
+    dims = (20, 12, 10)
+    vox = [sinusoid_field(dims, seed=s) for s in (21, 22, 23)]
+    ref = oracle.OracleVolume.dense_volume(vox)
+    vol = vkl.structured_regular(device, vox)
+    smp = vkl.Sampler(vol)
+    pts = _pts_around(dims, 16, seed=9, pad=-1.0)
+    attrs = [2, 0, 1, 2]
+    for w in (4, 8, 16):
+        valid = (np.arange(w) % 4 != 2).astype(np.int32)
+        got = smp.sample_m_w(pts[:w], attrs, valid=valid)
+        for m, a in enumerate(attrs):
+            np.testing.assert_array_equal(bits(got[m][valid == 1]), bits(ref.sample(pts[:w], attr=a)[valid == 1]))
+        assert np.isnan(got[:, valid == 0]).all()
 
 
 def test_shared_device_buffer_and_strided_host_data(vkl, device, oracle):
