@@ -348,6 +348,8 @@ void vklDeviceSetInt(VKLDevice dev, const char *name, int x)
     d->logLevel = x;
   if (!std::strcmp(name, "binnedSampling"))
     d->binning = x != 0;
+  if (!std::strcmp(name, "textureSampling"))
+    d->textureSampling = x != 0;
 }
 
 void vklDeviceSetString(VKLDevice dev, const char *name, const char *s)

@@ -147,6 +147,13 @@ struct DevGrid {
   // VdbLeafAccessObserver_observe (unsynchronised stores of the same value).
   uint32_t numLeafAccess;
   uint32_t *leafAccess[kMaxLeafObservers];
+  // Dense float attributes: texture object (0 = none) over a 2D atlas of the
+  // attribute's z-planes, plane z at texel (X * (z % atlasPlanesPerRow),
+  // Y * (z / atlasPlanesPerRow)).  The trilinear tile kernels fetch their
+  // 2x2x2 corners from it with two tld4 footprint gathers; z-neighbours sit
+  // side by side in the atlas, a few KB apart.
+  uint64_t atlasTex[kMaxAttributes];
+  uint32_t atlasPlanesPerRow;
 };
 
 struct DevSampler {

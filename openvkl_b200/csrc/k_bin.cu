@@ -275,8 +275,12 @@ BinGrid binGridOf(const DevGrid &g)
 
 bool binnedSamplingApplies(const DevGrid &g, int filter, uint64_t n, uint32_t attr)
 {
-  (void)filter;
   if (!g.dense || g.type[attr] != kFloat || n < kBinMinPts)
+    return false;
+  // trilinear taps from a texture atlas need no binning: the texture path
+  // takes incoherent points faster unsorted (16.6 vs 13-14 Gsamples/s on
+  // 2^26 random points of a 1024^3 volume)
+  if (filter == kFilterLinear && g.atlasTex[attr])
     return false;
   const uint64_t voxels = (uint64_t)g.activeSize[0] * g.activeSize[1] * g.activeSize[2];
   return voxels * 4 >= kBinMinVoxelBytes;

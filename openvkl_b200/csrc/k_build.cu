@@ -203,14 +203,30 @@ __device__ __forceinline__ TileCoords tileCoords(uint3 dims, uint3 nl)
 // x = X0 + (tid & 31), rows y = Y0 + (tid >> 5) + 8u.  brickIndex is a sum
 // of per-axis terms, so the x and y terms are computed once per thread and
 // the z term once per plane.
+// Texture atlas of a float attribute (DevGrid::atlasTex), written through a
+// surface object in the same pass; surf = 0: none.
+struct AtlasTarget {
+  uint64_t surf;
+  uint32_t planesPerRow;
+  uint32_t *denormal;  // set to 1 when a voxel is denormal (the texture path would flush it)
+};
+
+__device__ __forceinline__ bool isDenormal(float v)
+{
+  const uint32_t b = __float_as_uint(v);
+  return (b & 0x7f800000u) == 0 && (b & 0x007fffffu) != 0;
+}
+
 struct BrickWriter {
   uint64_t termXY[4];
   uint32_t valid;  // bit u: (x, y_u) inside the volume
   uint64_t zStride;
+  uint32_t x, y0;
 
   __device__ __forceinline__ BrickWriter(const TileCoords &t, uint32_t superX, uint32_t superY)
   {
-    const uint32_t x = (uint32_t)(t.X0 + (threadIdx.x & 31));
+    x  = (uint32_t)(t.X0 + (threadIdx.x & 31));
+    y0 = (uint32_t)(t.Y0 + (threadIdx.x >> 5));
     const uint64_t tx = ((uint64_t)(x >> 6) << 18) + (((x >> 3) & 7u) << 9) + (x & 7u);
     const uint64_t yStride = (uint64_t)superX << 18;
     zStride = (uint64_t)superX * superY << 18;
@@ -224,13 +240,25 @@ struct BrickWriter {
     }
   }
   template <typename T, class At>
-  __device__ __forceinline__ void write(uint32_t z, At at, T *__restrict__ dst) const
+  __device__ __forceinline__ void write(uint32_t z, At at, T *__restrict__ dst, const AtlasTarget &atlas,
+                                        const TileCoords &t, uint32_t &denormal) const
   {
     const uint64_t tz = (uint64_t)(z >> 6) * zStride + ((((z >> 3) & 7u) << 15) + ((z & 7u) << 6));
 #pragma unroll
     for (int u = 0; u < 4; ++u)
-      if (valid & (1u << u))
-        dst[termXY[u] + tz] = at((threadIdx.x >> 5) + 8 * u + 1, (threadIdx.x & 31) + 1);
+      if (valid & (1u << u)) {
+        const T v = at((threadIdx.x >> 5) + 8 * u + 1, (threadIdx.x & 31) + 1);
+        dst[termXY[u] + tz] = v;
+        if constexpr (std::is_same<T, float>::value) {
+          if (atlas.surf) {
+            const uint32_t ax = (z % atlas.planesPerRow) * (uint32_t)t.X + x,
+                           ay = (z / atlas.planesPerRow) * (uint32_t)t.Y + y0 + 8 * u;
+            surf2Dwrite(v, (cudaSurfaceObject_t)atlas.surf, (int)(ax * sizeof(float)), (int)ay,
+                        cudaBoundaryModeZero);
+            denormal |= isDenormal(v) ? 1u : 0u;
+          }
+        }
+      }
   }
 };
 
@@ -238,11 +266,12 @@ struct BrickWriter {
 // leaf x-windows (into xres).
 template <typename T, class At>
 __device__ __forceinline__ void planeRows(const TileCoords &t, int32_t z, At at, T *__restrict__ dst,
-                                          const BrickWriter &bw, PartialRange (*xres)[4])
+                                          const BrickWriter &bw, const AtlasTarget &atlas, uint32_t &denormal,
+                                          PartialRange (*xres)[4])
 {
   const int tid = threadIdx.x;
   if (z >= 8 * t.k0 && z < 8 * t.k1)
-    bw.write((uint32_t)z, at, dst);
+    bw.write((uint32_t)z, at, dst, atlas, t, denormal);
   if (tid < kPlaneW * 4) {
     const int r = tid >> 2, i = tid & 3;
     const int32_t y = t.Y0 - 1 + r;
@@ -319,7 +348,8 @@ __device__ __forceinline__ void finishLeaves(const TileCoords &t, const PartialR
 template <typename T>
 __global__ void __launch_bounds__(256, 4) kDenseBrickRanges(const T *__restrict__ src, T *__restrict__ dst,
                                                          uint3 dims, uint3 nl, uint32_t superX, uint32_t superY,
-                                                         float bg, float *__restrict__ leafRanges)
+                                                         float bg, float *__restrict__ leafRanges,
+                                                         AtlasTarget atlas)
 {
   __shared__ T plane[kPlaneW][kPlaneW];
   __shared__ PartialRange xres[kPlaneW][4];
@@ -327,6 +357,7 @@ __global__ void __launch_bounds__(256, 4) kDenseBrickRanges(const T *__restrict_
   const int tid        = threadIdx.x;
   const TileCoords t   = tileCoords(dims, nl);
   const BrickWriter bw(t, superX, superY);
+  uint32_t denormal = 0;
   // Loads: 245 threads = 7 rows x 35 columns per pass, 5 passes cover the
   // 35 rows.  A thread's column and its row validity are fixed; its voxel
   // offset within a plane is rowOff + 7 * u * X.
@@ -361,11 +392,12 @@ __global__ void __launch_bounds__(256, 4) kDenseBrickRanges(const T *__restrict_
     __syncthreads();
     if (z + 1 < t.zEnd)
       loadPlane(z + 1);
-    planeRows(t, z, at, dst, bw, xres);
+    planeRows(t, z, at, dst, bw, atlas, denormal, xres);
     __syncthreads();
     planeColumns(xres, pres[z - t.zBeg]);
   }
-  __syncthreads();
+  if (__syncthreads_or(denormal) && tid == 0)
+    atomicOr(atlas.denormal, 1u);
   finishLeaves(t, pres, src, dims, nl, bg, leafRanges);
 }
 
@@ -630,14 +662,16 @@ void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint
 
 void launchDenseBrickRanges(const void *src, uint32_t type, void *dst, const uint32_t dims[3],
                             uint32_t superX, uint32_t superY, float background, float *leafRanges,
+                            uint64_t atlasSurface, uint32_t atlasPlanesPerRow, uint32_t *denormalFlag,
                             cudaStream_t st)
 {
+  const AtlasTarget atlas{type == kFloat ? atlasSurface : 0, atlasPlanesPerRow, denormalFlag};
   const uint3 D  = {dims[0], dims[1], dims[2]};
   const uint3 NL = {(dims[0] + 7) / 8, (dims[1] + 7) / 8, (dims[2] + 7) / 8};
   const dim3 grid((NL.x + 3) / 4, (NL.y + 3) / 4, (NL.z + kDenseChunk - 1) / kDenseChunk);
 #define VKL_DENSE_BRICK(T)                                                                              \
   kDenseBrickRanges<T><<<grid, 256, 0, st>>>((const T *)src, (T *)dst, D, NL, superX, superY, background, \
-                                             leafRanges)
+                                             leafRanges, atlas)
   switch (type) {
   case kUChar:
     VKL_DENSE_BRICK(uint8_t);

@@ -40,9 +40,13 @@ void launchBuildDenseTree(const DevGrid &g, uint64_t *vox0, uint64_t *vox1, uint
 // Dense commit of one attribute: writes the bricked copy of the x-fastest
 // voxel array `src` (element type `type`, kUChar..kDouble) to `dst`, and the
 // per-leaf value ranges (2 floats per leaf, leaves x-fastest) over each
-// leaf's 3x3x3-leaf filter neighbourhood window.
+// leaf's 3x3x3-leaf filter neighbourhood window.  For a float attribute with
+// `atlasSurface` != 0 it also writes the z-plane texture atlas (DevGrid::
+// atlasTex) through that surface and sets *denormalFlag (a device word the
+// caller zeroes) to 1 if any voxel is denormal.
 void launchDenseBrickRanges(const void *src, uint32_t type, void *dst, const uint32_t dims[3],
                             uint32_t superX, uint32_t superY, float background, float *leafRanges,
+                            uint64_t atlasSurface, uint32_t atlasPlanesPerRow, uint32_t *denormalFlag,
                             cudaStream_t stream);
 // Same for sparse volumes, leaves given by root-relative offsets (3 u32).
 void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,

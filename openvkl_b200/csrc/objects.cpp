@@ -347,6 +347,111 @@ uint64_t packKey(uint32_t x, uint32_t y, uint32_t z)
 
 }  // namespace
 
+void TextureAtlas::release()
+{
+  if (tex)
+    cudaDestroyTextureObject(tex);
+  if (surf)
+    cudaDestroySurfaceObject(surf);
+  if (array)
+    cudaFreeArray(array);
+  tex = surf = 0;
+  array = nullptr;
+  width = height = 0;
+}
+
+bool TextureAtlas::ensure(uint32_t w, uint32_t h)
+{
+  if (array && w == width && h == height)
+    return true;
+  release();
+  cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
+  if (cudaMallocArray(&array, &fmt, w, h, cudaArraySurfaceLoadStore) != cudaSuccess) {
+    cudaGetLastError();  // an atlas that does not fit is skipped, not an error
+    array = nullptr;
+    return false;
+  }
+  cudaResourceDesc res{};
+  res.resType         = cudaResourceTypeArray;
+  res.res.array.array = array;
+  cudaTextureDesc td{};
+  td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
+  td.filterMode       = cudaFilterModePoint;
+  td.readMode         = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  cudaCheck(cudaCreateSurfaceObject(&surf, &res), "atlas surface");
+  cudaCheck(cudaCreateTextureObject(&tex, &res, &td, nullptr), "atlas texture");
+  width  = w;
+  height = h;
+  return true;
+}
+
+std::unique_ptr<TextureAtlas> Device::takeAtlas(uint32_t width, uint32_t height)
+{
+  std::lock_guard<std::mutex> lock(atlasMutex);
+  for (auto it = atlasPool.begin(); it != atlasPool.end(); ++it)
+    if ((*it)->width == width && (*it)->height == height) {
+      std::unique_ptr<TextureAtlas> a = std::move(*it);
+      atlasPool.erase(it);
+      return a;
+    }
+  return nullptr;
+}
+
+void Device::giveAtlas(std::unique_ptr<TextureAtlas> atlas)
+{
+  if (!atlas || !atlas->array)
+    return;
+  std::lock_guard<std::mutex> lock(atlasMutex);
+  atlasPool.push_back(std::move(atlas));
+  while (atlasPool.size() > kAtlasPool)
+    atlasPool.erase(atlasPool.begin());
+}
+
+void Device::dropAtlases()
+{
+  std::lock_guard<std::mutex> lock(atlasMutex);
+  atlasPool.clear();
+}
+
+Volume::~Volume()
+{
+  for (auto &a : atlases)
+    if (a && device)
+      device->giveAtlas(std::move(a));
+}
+
+namespace {
+
+// Planes per atlas row for X x Y x Z float planes within the device's 2D
+// texture and surface limits; 0 when the volume does not fit one atlas.
+// Up to 64 planes side by side keep z-neighbours a few KB apart.
+uint32_t atlasPlanesPerRow(int cudaDevice, uint32_t X, uint32_t Y, uint32_t Z)
+{
+  int tw = 0, th = 0, sw = 0, sh = 0;
+  cudaDeviceGetAttribute(&tw, cudaDevAttrMaxTexture2DWidth, cudaDevice);
+  cudaDeviceGetAttribute(&th, cudaDevAttrMaxTexture2DHeight, cudaDevice);
+  cudaDeviceGetAttribute(&sw, cudaDevAttrMaxSurface2DWidth, cudaDevice);
+  cudaDeviceGetAttribute(&sh, cudaDevAttrMaxSurface2DHeight, cudaDevice);
+  const uint64_t maxW = (uint64_t)std::min(tw, sw), maxH = (uint64_t)std::min(th, sh);
+  uint64_t T = std::min<uint64_t>(Z, 64);
+  if (T * X > maxW)
+    T = maxW / X;
+  if (T == 0)
+    return 0;
+  if ((Z + T - 1) / T * Y > maxH) {
+    const uint64_t rowsMax = maxH / Y;
+    if (rowsMax == 0)
+      return 0;
+    T = (Z + rowsMax - 1) / rowsMax;
+    if (T * X > maxW)
+      return 0;
+  }
+  return (uint32_t)T;
+}
+
+}  // namespace
+
 void Volume::commit()
 {
   // Work that still reads the previous commit's buffers (on any stream)
@@ -510,9 +615,17 @@ void Volume::commitDense()
   // checked against the domain first).
   // leaf ranges and the volume range: scratch of the commit, kept with the
   // volume so that a re-commit reuses them
-  DeviceBuffer &leafRanges = *newBuffer(grid.numLeaves * 8), &volRange = *newBuffer(8 * NA);
+  // volRange also holds one denormal flag per attribute after the ranges.
+  DeviceBuffer &leafRanges = *newBuffer(grid.numLeaves * 8), &volRange = *newBuffer(12 * NA);
+  uint32_t *denormalFlags  = (uint32_t *)(volRange.as<float>() + 2 * NA);
+  cudaCheck(cudaMemsetAsync(denormalFlags, 0, 4 * NA, st), "memset");
   const uint32_t udims[3] = {(uint32_t)dims[0], (uint32_t)dims[1], (uint32_t)dims[2]};
   const uint64_t nb       = brickedElements(udims, grid.superX, grid.superY);
+  // Texture atlases of float attributes (trilinear sampling through tld4):
+  // planes side by side, written by the commit pass itself.
+  const uint32_t planesPerRow =
+      device->textureSampling ? atlasPlanesPerRow(device->cudaDevice, udims[0], udims[1], udims[2]) : 0;
+  grid.atlasPlanesPerRow = planesPerRow ? planesPerRow : 1;
   for (uint32_t a = 0; a < grid.numAttributes; ++a) {
     const size_t es  = sizeOfType(attrs[a]->type);
     DeviceBuffer *bb = newBuffer(nb * es);
@@ -520,15 +633,45 @@ void Volume::commitDense()
       cudaCheck(cudaMemsetAsync(bb->ptr, 0, nb * es, st), "memset");
     grid.data[a] = bb->ptr;
     grid.type[a] = attrs[a]->type;
+    uint64_t surf = 0;
+    if (planesPerRow && attrs[a]->type == VKL_FLOAT) {
+      const uint32_t w = planesPerRow * udims[0], h = (udims[2] + planesPerRow - 1) / planesPerRow * udims[1];
+      if (atlases[a] && (atlases[a]->width != w || atlases[a]->height != h))
+        device->giveAtlas(std::move(atlases[a]));
+      if (!atlases[a])
+        atlases[a] = device->takeAtlas(w, h);
+      if (!atlases[a])
+        atlases[a].reset(new TextureAtlas());
+      bool ok = atlases[a]->ensure(w, h);
+      if (!ok) {  // memory held by pooled atlases first
+        device->dropAtlases();
+        ok = atlases[a]->ensure(w, h);
+      }
+      if (ok)
+        surf = atlases[a]->surf;
+    } else if (atlases[a]) {
+      device->giveAtlas(std::move(atlases[a]));
+    }
     launchDenseBrickRanges(attrs[a]->dev, attrs[a]->type, bb->ptr, udims, grid.superX, grid.superY,
-                           grid.background[a], leafRanges.as<float>(), st);
+                           grid.background[a], leafRanges.as<float>(), surf, grid.atlasPlanesPerRow,
+                           denormalFlags + a, st);
     launchPropagateRanges(grid, a, grid.numLeaves, nullptr, leafRanges.as<float>(),
                           volRange.as<float>() + 2 * a, nl, st);
   }
-  std::vector<float> vr(2 * NA);
-  cudaCheck(cudaMemcpyAsync(vr.data(), volRange.ptr, 8 * NA, cudaMemcpyDeviceToHost, st),
+  std::vector<float> vr(3 * NA);
+  cudaCheck(cudaMemcpyAsync(vr.data(), volRange.ptr, 12 * NA, cudaMemcpyDeviceToHost, st),
             "value range readback");
   cudaCheck(cudaStreamSynchronize(st), "dense commit");
+  // an attribute with denormal voxels is sampled without its atlas (the
+  // texture path would flush them to zero)
+  for (uint32_t a = 0; a < NA; ++a) {
+    uint32_t denormal = 0;
+    std::memcpy(&denormal, &vr[2 * NA + a], 4);
+    if (atlases[a] && atlases[a]->array && !denormal)
+      grid.atlasTex[a] = atlases[a]->tex;
+    else if (atlases[a])
+      device->giveAtlas(std::move(atlases[a]));
+  }
   rangeLo.assign(NA, 0);
   rangeHi.assign(NA, 0);
   for (uint32_t a = 0; a < NA; ++a) {

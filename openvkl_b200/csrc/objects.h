@@ -175,6 +175,8 @@ bool binnedSamplingApplies(const DevGrid &g, int filter, uint64_t n, uint32_t at
 bool launchSampleBinned(const DevGrid &g, int filter, uint64_t n, const float *pts, uint32_t attr,
                         float *out, bool grad, BinScratch &scratch, cudaStream_t stream);
 
+struct TextureAtlas;
+
 struct Device {
   int cudaDevice = 0;
   cudaStream_t stream = nullptr;
@@ -210,6 +212,20 @@ struct Device {
   std::mutex binMutex;
   BinScratch binScratch;
   bool binning = true;
+  // Texture atlases of dense float attributes (DevGrid::atlasTex): on by
+  // default; device parameter "textureSampling" 0 turns them off for volumes
+  // committed afterwards.
+  bool textureSampling = true;
+  // Atlases of released or re-shaped volumes, kept for the next commit of
+  // an atlas of the same size (a volume released and created again each
+  // frame then allocates none); at most kAtlasPool are kept, and all are
+  // dropped when an atlas allocation fails.
+  static constexpr size_t kAtlasPool = 2;
+  std::mutex atlasMutex;
+  std::vector<std::unique_ptr<TextureAtlas>> atlasPool;
+  std::unique_ptr<TextureAtlas> takeAtlas(uint32_t width, uint32_t height);
+  void giveAtlas(std::unique_ptr<TextureAtlas> atlas);
+  void dropAtlases();
 
   void setError(VKLError code, const std::string &msg);
   void log(int level, const std::string &msg);
@@ -241,6 +257,27 @@ struct Data : ManagedObject {
 };
 
 // ---------------------------------------------------------------------------
+// 2D float texture atlas of one dense attribute's z-planes (DevGrid::
+// atlasTex): a cudaArray written through a surface object at commit and
+// read through a texture object (point sampling, unnormalized coordinates,
+// border addressing).
+// ---------------------------------------------------------------------------
+struct TextureAtlas {
+  cudaArray_t array        = nullptr;
+  cudaSurfaceObject_t surf = 0;
+  cudaTextureObject_t tex  = 0;
+  uint32_t width = 0, height = 0;
+  TextureAtlas() = default;
+  TextureAtlas(const TextureAtlas &) = delete;
+  TextureAtlas &operator=(const TextureAtlas &) = delete;
+  ~TextureAtlas() { release(); }
+  void release();
+  // Creates (or keeps, if the size is unchanged) a width x height atlas;
+  // false if the device cannot allocate it.
+  bool ensure(uint32_t w, uint32_t h);
+};
+
+// ---------------------------------------------------------------------------
 // Volumes.
 // ---------------------------------------------------------------------------
 struct Volume : ManagedObject {
@@ -258,6 +295,8 @@ struct Volume : ManagedObject {
 
   const char *typeName() const override { return isDense ? "structuredRegular" : "vdb"; }
   void commit() override;
+  ~Volume() override;
+  std::unique_ptr<TextureAtlas> atlases[kMaxAttributes];
   // Device buffers of the previous commit.  A re-commit takes buffers of
   // the sizes it needs from here (a time-varying volume re-committed with
   // new data of the same shape allocates nothing); the rest are freed when

@@ -23,11 +23,12 @@ __device__ __forceinline__ f3 loadPoint(const float *__restrict__ pts, uint64_t 
 template <class Field, int FILTER>
 __device__ __forceinline__ float filterAt(const Field &F, bool cc, f3 p)
 {
-  if (FILTER == kFilterNearest)
+  if constexpr (FILTER == kFilterNearest)
     return sampleNearest(F, cc, p);
-  if (FILTER == kFilterCubic)
+  else if constexpr (FILTER == kFilterCubic)
     return sampleCubic(F, p);
-  return sampleLinear(F, p);
+  else
+    return sampleLinear(F, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -54,6 +55,10 @@ __device__ __forceinline__ SparseField<T> makeFieldAs(const DevGrid &g, uint32_t
                                                       SparseField<T> *)
 {
   return SparseField<T>(g, a, depth);
+}
+__device__ __forceinline__ AtlasField makeFieldAs(const DevGrid &g, uint32_t a, uint32_t, AtlasField *)
+{
+  return AtlasField(g, a);
 }
 template <class Field>
 __device__ __forceinline__ Field makeField(const DevGrid &g, uint32_t attr, uint32_t maxDepth)
@@ -99,9 +104,14 @@ __device__ __forceinline__ void tileScan(int *hist)
 // The tricubic instances are held to two CTAs per SM (128 registers, a few
 // spilled): the extra resident warps hide more of the 64-tap stencil's load
 // latency than the spills cost (8.8 vs 8.2 Gsamples/s on the coherent
-// 1024^3 workload).
-template <typename T, bool DENSE, int FILTER, bool GRAD, int TILE>
-__global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : 1)
+// 1024^3 workload).  The texture-atlas instances are held to four (64
+// registers): they are bound by gather latency, and the fourth CTA gives
+// 90.7 vs 84 Gsamples/s on the coherent workload (16.6 vs 17.5 on random
+// points).
+// ATLAS: a dense float attribute's corners come from its texture atlas
+// (AtlasField, trilinear only).
+template <typename T, bool DENSE, int FILTER, bool GRAD, int TILE, bool ATLAS = false>
+__global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : (ATLAS ? 4 : 1))
     kSampleTile(const __grid_constant__ DevGrid g, uint32_t maxDepth, uint64_t n, const float *__restrict__ pts,
                 uint32_t attr, float *__restrict__ out)
 {
@@ -161,7 +171,8 @@ __global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : 1)
   __syncthreads();
   const bool cc = g.constantCellData != 0;
   // field parameters read from the launch's constant bank once per thread
-  using Field = typename std::conditional<DENSE, DenseField<T>, SparseField<T>>::type;
+  using Field = typename std::conditional<
+      ATLAS, AtlasField, typename std::conditional<DENSE, DenseField<T>, SparseField<T>>::type>::type;
   const Field F = makeField<Field>(g, attr, maxDepth);
   auto compute = [&](int j) {
     const int k = threadIdx.x + j * kTileThreads;
@@ -171,10 +182,10 @@ __global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : 1)
       const int o    = __float_as_int(e.w);
       if (GRAD) {
         f3 r = {0.f, 0.f, 0.f};
-        if (FILTER != kFilterNearest) {
-          const f3 gi = FILTER == kFilterCubic ? gradientCubic(F, q) : gradientLinear(F, q);
-          r = xfmNormal(g.objectToIndex, gi);
-        }
+        if constexpr (FILTER == kFilterCubic)
+          r = xfmNormal(g.objectToIndex, gradientCubic(F, q));
+        else if constexpr (FILTER == kFilterLinear)
+          r = xfmNormal(g.objectToIndex, gradientLinear(F, q));
         res[3 * o]     = r.x;
         res[3 * o + 1] = r.y;
         res[3 * o + 2] = r.z;
@@ -205,6 +216,20 @@ void launchTyped(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float *p
 {
   // 2048-point tiles for samples (44 KB shared), 1024 for gradients and the
   // register-heavy tricubic.
+  if constexpr (DENSE && FILTER == kFilterLinear && std::is_same<T, float>::value) {
+    if (g.atlasTex[attr]) {
+      if (grad) {
+        constexpr int TILE = 1024;
+        kSampleTile<T, true, FILTER, true, TILE, true>
+            <<<(unsigned)((n + TILE - 1) / TILE), kTileThreads, 0, st>>>(g, maxDepth, n, pts, attr, out);
+      } else {
+        constexpr int TILE = 2048;
+        kSampleTile<T, true, FILTER, false, TILE, true>
+            <<<(unsigned)((n + TILE - 1) / TILE), kTileThreads, 0, st>>>(g, maxDepth, n, pts, attr, out);
+      }
+      return;
+    }
+  }
   if (grad) {
     constexpr int TILE = 1024;
     kSampleTile<T, DENSE, FILTER, true, TILE>

@@ -212,6 +212,68 @@ struct DenseField {
 };
 
 // ---------------------------------------------------------------------------
+// Dense float attribute read through its z-plane texture atlas (DevGrid::
+// atlasTex): the 8 trilinear corners are two tld4 footprint gathers, one per
+// z-plane, instead of 8 loads through the L1 load/store pipe.  Point
+// sampling returns the stored bits of every non-denormal float; the commit
+// builds the atlas only for attributes without denormals, so the corners are
+// the DenseField's.  Corners outside the domain read the background like
+// DenseField::stencil: every lane issues both gathers and selects.
+// tld4 returns the footprint (u0,v0)..(u1,v1), u0 = floor(u - 0.5), as
+// .x (u0,v1)  .y (u1,v1)  .z (u1,v0)  .w (u0,v0).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 tld4Red(uint64_t tex, float u, float v)
+{
+  float4 r;
+  asm volatile("tld4.r.2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6}];"
+               : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+               : "l"(tex), "f"(u), "f"(v));
+  return r;
+}
+
+struct AtlasField {
+  uint64_t tex;
+  uint32_t ax, ay, az;
+  int32_t rx, ry, rz;
+  uint32_t planesPerRow;
+  float bg;
+
+  __device__ __forceinline__ AtlasField(const DevGrid &g, uint32_t a)
+      : tex(g.atlasTex[a]),
+        ax(g.activeSize[0]),
+        ay(g.activeSize[1]),
+        az(g.activeSize[2]),
+        rx(g.rootOrigin[0]),
+        ry(g.rootOrigin[1]),
+        rz(g.rootOrigin[2]),
+        planesPerRow(g.atlasPlanesPerRow),
+        bg(g.background[a])
+  {
+  }
+
+  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  {
+    const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
+    const bool vx0 = ox < ax, vx1 = ox + 1u < ax, vy0 = oy < ay, vy1 = oy + 1u < ay, vz0 = oz < az,
+               vz1 = oz + 1u < az;
+    // footprint origin inside the plane's tile: (ox, oy) when valid, else
+    // (-1, -1) relative (only the +1 corner can be in the domain then)
+    const float fx = vx0 ? (float)(ox + 1u) : 0.f, fy = vy0 ? (float)(oy + 1u) : 0.f;
+    const uint32_t z0 = vz0 ? oz : 0u, z1 = vz1 ? oz + 1u : 0u;
+    const float4 a = tld4Red(tex, (float)((z0 % planesPerRow) * ax) + fx, (float)((z0 / planesPerRow) * ay) + fy);
+    const float4 b = tld4Red(tex, (float)((z1 % planesPerRow) * ax) + fx, (float)((z1 / planesPerRow) * ay) + fy);
+    s[0] = (vx0 & vy0 & vz0) ? a.w : bg;
+    s[1] = (vx0 & vy0 & vz1) ? b.w : bg;
+    s[2] = (vx0 & vy1 & vz0) ? a.x : bg;
+    s[3] = (vx0 & vy1 & vz1) ? b.x : bg;
+    s[4] = (vx1 & vy0 & vz0) ? a.z : bg;
+    s[5] = (vx1 & vy0 & vz1) ? b.z : bg;
+    s[6] = (vx1 & vy1 & vz0) ? a.y : bg;
+    s[7] = (vx1 & vy1 & vz1) ? b.y : bg;
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Leaf codecs of sparse volumes.  T = float / __half: the leaf arrays hold the
 // values.  The Code* tags: compressed leaves (an extension, no reference
 // counterpart) hold FP16 / BF16 / FP8-E4M3 codes, value = code * scale +

@@ -205,3 +205,58 @@ def test_chunked_host_pointer_calls(vkl, device, where):
     as_np = lambda t: t.cpu().numpy() if hasattr(t, "cpu") else t
     np.testing.assert_array_equal(bits(as_np(got_s)), bits(want_s.cpu().numpy()))
     np.testing.assert_array_equal(bits(as_np(got_g)), bits(want_g.cpu().numpy()))
+
+
+def _atlas_cases(vkl, device_on, device_off, oracle, vox, **kw):
+    """Samples and gradients of one float volume committed with the texture
+    atlas (device_on) and without it (device_off), against the oracle."""
+    ref = oracle.OracleVolume.dense_volume(vox, **kw)
+    on = vkl.structured_regular(device_on, vox, **kw)
+    off = vkl.structured_regular(device_off, vox, **kw)
+    return ref, on, off
+
+
+@pytest.mark.parametrize("case", ["plain", "index_origin", "cell_centered", "transform"])
+def test_texture_atlas_bit_exact(vkl, oracle, case):
+    """Trilinear samples and gradients of dense float volumes read through
+    the z-plane texture atlas (tld4 footprint gathers) equal the bricked
+    loads' and the oracle's bit for bit, inside, on the faces and outside
+    the domain, for odd dims, index origins, cell-centered data, background
+    values and a rotated transform."""
+    on, off = vkl.Device("cuda"), vkl.Device("cuda")
+    off.set_int("textureSampling", 0)
+    dims = (67, 45, 33)
+    vox = sinusoid_field(dims, seed=31)
+    kw = {"plain": {}, "index_origin": {"index_origin": (-3, 2, 5), "background": [-1.5]},
+          "cell_centered": {"cell_centered": True, "background": [0.25]},
+          "transform": {"index_to_object": [0.8, 0.6, 0, -0.6, 0.8, 0, 0, 0, 1.25, 3.0, -2.0, 1.0]}}[case]
+    ref, von, voff = _atlas_cases(vkl, on, off, oracle, vox, **kw)
+    b = np.array(von.bounding_box(), np.float64)
+    pts = uniform_points(200000, b[:3] - 2, b[3:] + 2, seed=32)
+    for fv in (100,):
+        son, soff = vkl.Sampler(von, filter=fv, gradient_filter=fv), vkl.Sampler(voff, filter=fv, gradient_filter=fv)
+        want = ref.sample(pts, filter=fv)
+        np.testing.assert_array_equal(bits(son.sample(pts)), bits(want))
+        np.testing.assert_array_equal(bits(soff.sample(pts)), bits(want))
+        gw = ref.gradient(pts, filter=fv)
+        np.testing.assert_array_equal(bits(son.gradient(pts)), bits(gw))
+        np.testing.assert_array_equal(bits(soff.gradient(pts)), bits(gw))
+
+
+def test_texture_atlas_skipped_for_denormals(vkl, oracle):
+    """The texture path flushes denormals to zero, so a float attribute with
+    denormal voxels is sampled from the bricked copy: results stay the
+    oracle's.  A second, denormal-free attribute of the same volume keeps
+    its atlas."""
+    on = vkl.Device("cuda")
+    dims = (40, 36, 30)
+    a = sinusoid_field(dims, seed=33) * np.float32(1e-37)  # many results below FLT_MIN
+    a.reshape(-1)[::7] = np.float32(3e-39)  # denormal voxels
+    b = sinusoid_field(dims, seed=34)
+    ref = oracle.OracleVolume.dense_volume([a, b])
+    vol = vkl.structured_regular(on, [a, b])
+    smp = vkl.Sampler(vol)
+    pts = uniform_points(100000, (-1, -1, -1), (40, 36, 30), seed=35)
+    for attr in (0, 1):
+        np.testing.assert_array_equal(bits(smp.sample(pts, attr=attr)), bits(ref.sample(pts, attr=attr)))
+    assert (np.abs(ref.sample(pts, attr=0)) < np.float32(1.1754944e-38)).any()
