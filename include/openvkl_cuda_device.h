@@ -93,12 +93,23 @@ __device__ __forceinline__ auto withField(const DevGrid &g, uint32_t attr, uint3
   return f(SparseField<float>(g, attr, depth));
 }
 
+// A dense float attribute with a texture atlas samples its trilinear corners
+// from it (AtlasField): the same bits as the bricked loads.
+__device__ __forceinline__ bool atlasLinear(const DevGrid &g, int filter, uint32_t attr, VKLFeatureFlags ff,
+                                            VKLFeatureFlags filterBit)
+{
+  return (ff & kStructuredRegular) && (ff & filterBit) && filter == kFilterLinear && g.dense &&
+         g.atlasTex[attr] != 0;
+}
+
 __device__ __forceinline__ float sample(const DevGrid &g, int filter, uint32_t depth, uint32_t attr, f3 oc,
                                         VKLFeatureFlags ff)
 {
   if (ff == 0)
     ff = ~0ull;
   const f3 p    = xfmPoint(g.objectToIndex, oc);
+  if (atlasLinear(g, filter, attr, ff, kSampleLinear))
+    return sampleLinear(AtlasField(g, attr), p);
   const bool cc = g.constantCellData != 0;
   return withField(g, attr, depth, ff, [&](const auto &F) -> float {
     if ((ff & kSampleNearest) && filter == kFilterNearest)
@@ -118,6 +129,8 @@ __device__ __forceinline__ f3 gradient(const DevSamplerState *st, uint32_t attr,
   if ((ff & kGradientNearest) && filter == kFilterNearest)
     return {0.f, 0.f, 0.f};
   const f3 p = xfmPoint(g.objectToIndex, oc);
+  if (atlasLinear(g, filter, attr, ff, kGradientLinear))
+    return xfmNormal(g.objectToIndex, gradientLinear(AtlasField(g, attr), p));
   return withField(g, attr, st->s.maxSamplingDepth, ff, [&](const auto &F) -> f3 {
     const f3 gi = ((ff & kGradientCubic) && filter == kFilterCubic) ? gradientCubic(F, p) : gradientLinear(F, p);
     return xfmNormal(g.objectToIndex, gi);
