@@ -649,8 +649,8 @@ def run_intervals(args):
     line = {"metric": METRIC, "value": n / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "dtype": "f32", "data": "synthetic (seeded sinusoid volume, generated rays)",
-            "config": {"workload": "interval iterator, structuredRegular 1024^3 float32, 1920x1080 orbit-camera "
-                                   "rays, 4 value ranges (quartiles), default resolution hint",
+            "config": {"workload": f"interval iterator, structuredRegular {DIMS[0]}^3 float32, {WIDTH}x{HEIGHT} "
+                                   "orbit-camera rays, 4 value ranges (quartiles), default resolution hint",
                        "rays": n, "intervals_per_step": total, "max_per_ray": m},
             "intervals_per_s": total / (ms * 1e-3),
             "roofline": {"bound": "latency (per-ray serial DDA)", "alg_bytes_per_launch": n * 32 + total * 20,
