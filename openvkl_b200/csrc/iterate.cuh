@@ -136,16 +136,18 @@ __device__ inline void queryVoxelDense(const DevGrid &g, int32_t x, int32_t y, i
     return;
   }
   // The reference computes the level-1/2 node numbers in closed form
-  // (z-major over the dense node grid, VdbQueryVoxelDense.ih:41-113); walking
-  // the child pointers gives the same voxel for every volume up to 4096^3
-  // and never indexes past a level's arrays beyond that.
+  // (VdbQueryVoxelDense.ih:41-113).  The dense tree numbers level-l nodes
+  // x-fastest over the node grid (k_build.cu kDenseLevel*), so the node of
+  // an in-domain cell is its node coordinates' linear index: the same voxel
+  // the child-pointer walk reaches, without its two dependent loads.
   const uint32_t lvl = depth >= 2 ? 2u : depth;
-  uint64_t node = 0, ni = 0;
-  for (uint32_t l = 0;; ++l) {
-    ni = node * levelNumVoxels(l) + offsetToLinear(l, ox, oy, oz);
-    if (l == lvl)
-      break;
-    node = voxelChildIndex(__ldg(g.levels[l].voxels + ni));
+  uint64_t ni = offsetToLinear(lvl, ox, oy, oz);
+  if (lvl == 2) {
+    const uint32_t n2x = (g.activeSize[0] + 127) >> 7, n2y = (g.activeSize[1] + 127) >> 7;
+    ni += (((uint64_t)(oz >> 7) * n2y + (oy >> 7)) * n2x + (ox >> 7)) * levelNumVoxels(2);
+  } else if (lvl == 1) {
+    const uint32_t n1x = (g.activeSize[0] + 4095) >> 12, n1y = (g.activeSize[1] + 4095) >> 12;
+    ni += (((uint64_t)(oz >> 12) * n1y + (oy >> 12)) * n1x + (ox >> 12)) * levelNumVoxels(1);
   }
   const float *r = g.levels[lvl].valueRange + 2 * (ni * g.numAttributes + attr);
   desc.v0        = __ldg(r);
