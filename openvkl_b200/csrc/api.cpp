@@ -66,6 +66,10 @@ T *objectAs(const VKLObject &o, const char *what)
 
 VKLObject handleOf(ManagedObject *o, void *dev = nullptr)
 {
+  if (o->device && !o->heldDevice) {
+    o->heldDevice = o->device;
+    o->heldDevice->refInc();
+  }
   VKLObject h;
   h.host   = o;
   h.device = dev;
@@ -423,10 +427,12 @@ void vklReleaseDevice(VKLDevice dev)
 {
   if (!dev)
     return;
-  std::lock_guard<std::mutex> lock(g_devicesMutex);
-  if (g_lastDevice == (Device *)dev)
-    g_lastDevice = nullptr;
-  delete (Device *)dev;
+  {
+    std::lock_guard<std::mutex> lock(g_devicesMutex);
+    if (g_lastDevice == (Device *)dev)
+      g_lastDevice = nullptr;
+  }
+  ((Device *)dev)->refDec();  // freed when its last object goes (vklReleaseDevice, API.cpp:298-303)
 }
 
 // ---------------------------------------------------------------------------

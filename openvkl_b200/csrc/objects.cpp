@@ -77,6 +77,14 @@ ManagedObject::~ManagedObject()
   for (auto &kv : params)
     if (kv.second.obj)
       kv.second.obj->refDec();
+  if (heldDevice)
+    heldDevice->refDec();
+}
+
+void Device::refDec()
+{
+  if (refs.fetch_sub(1) == 1)
+    delete this;
 }
 
 void ManagedObject::setParam(const char *name, VKLDataType type, const void *mem)

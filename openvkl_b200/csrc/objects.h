@@ -49,6 +49,10 @@ struct Device;
 struct ManagedObject {
   std::atomic<int> refs{1};
   Device *device = nullptr;
+  // The device this object keeps alive (taken when its handle is made,
+  // dropped when it is destroyed): as in the reference, vklReleaseDevice
+  // frees a device only once its objects are gone.
+  Device *heldDevice = nullptr;
 
   struct Param {
     VKLDataType type = VKL_UNKNOWN;
@@ -178,6 +182,10 @@ bool launchSampleBinned(const DevGrid &g, int filter, uint64_t n, const float *p
 struct TextureAtlas;
 
 struct Device {
+  // 1 for the application's handle plus 1 per live object of the device.
+  std::atomic<int> refs{1};
+  void refInc() { refs.fetch_add(1); }
+  void refDec();
   int cudaDevice = 0;
   cudaStream_t stream = nullptr;
   VKLError lastErrorCode = VKL_NO_ERROR;

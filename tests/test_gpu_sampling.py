@@ -260,3 +260,22 @@ def test_texture_atlas_skipped_for_denormals(vkl, oracle):
     for attr in (0, 1):
         np.testing.assert_array_equal(bits(smp.sample(pts, attr=attr)), bits(ref.sample(pts, attr=attr)))
     assert (np.abs(ref.sample(pts, attr=0)) < np.float32(1.1754944e-38)).any()
+
+
+def test_device_released_before_its_objects(vkl, oracle):
+    """vklReleaseDevice frees the device only once its objects are gone, as
+    in the reference (API.cpp:298-303, objects hold a reference to their
+    device): a volume and sampler keep working after the device's release,
+    and releasing them last frees it."""
+    dev = vkl.Device("cuda")
+    vox = sinusoid_field((40, 24, 20), seed=41)
+    ref = oracle.OracleVolume.dense_volume(vox)
+    vol = vkl.structured_regular(dev, vox)
+    smp = vkl.Sampler(vol)
+    pts = uniform_points(20000, (-1, -1, -1), (40, 24, 20), seed=42)
+    handle, dev.handle = dev.handle, None
+    dev.lib.vklReleaseDevice(handle)  # the application's handle goes first
+    np.testing.assert_array_equal(bits(smp.sample(pts)), bits(ref.sample(pts)))
+    np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts)))
+    smp.release()
+    vol.release()  # the last object: the device (and its atlas pool) go here
