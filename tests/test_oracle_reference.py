@@ -22,6 +22,9 @@ fields, tolerances and expected values:
 * InnerNode observer: node boxes contain their voxels and ranges contain the
   voxel values (vdb_volume_inner_node_observer.cpp:78-132)
 * commit errors of malformed VDB input (vdb_volume.cpp:17-79)
+* dense leaf value ranges equal a direct restatement of the reference's fold
+  order on volumes with NaN and -0.0 voxels (VdbSampler.ispc:460-557,
+  VdbSampler_dense.ih:35-105)
 """
 import json
 import math
@@ -252,3 +255,65 @@ def test_vdb_commit_errors(oracle):
                                        packed_tile=np.zeros(1, np.float32))
     with pytest.raises(RuntimeError, match="leaf nodes are only supported on the lowest level"):
         oracle.OracleVolume.vdb_volume([2], [[0, 0, 0]], [1], data)
+
+
+def _reference_fold_leaf_range(vox, ox, oy, oz, bg):
+    """One leaf's value range in the reference's own fold order, restated in
+    Python: the 27 neighbour windows [7,8) | [0,8) | [0,2) per axis in
+    neighbour order (x, y, z), voxels x outer / z inner, extend() as
+    (a < b ? a : b, a > b ? a : b) (so a NaN voxel resets the running
+    bound), a neighbour outside the domain contributing (bg, bg), and
+    neighbour bounds that are NaN skipped (VdbSampler.ispc:460-557,
+    VdbSampler_dense.ih:35-105)."""
+    Z, Y, X = vox.shape
+    win = [(7, 8), (0, 8), (0, 2)]
+    fmin = lambda a, b: a if a < b else b
+    fmax = lambda a, b: a if a > b else b
+    lo, hi = np.float32(np.inf), np.float32(-np.inf)
+    for ix in range(3):
+        for iy in range(3):
+            for iz in range(3):
+                nx, ny, nz = ox + (ix - 1) * 8, oy + (iy - 1) * 8, oz + (iz - 1) * 8
+                if not (0 <= nx < X and 0 <= ny < Y and 0 <= nz < Z):
+                    nlo = nhi = np.float32(bg)
+                else:
+                    nlo, nhi = np.float32(np.inf), np.float32(-np.inf)
+                    for x in range(*win[ix]):
+                        for y in range(*win[iy]):
+                            for z in range(*win[iz]):
+                                px, py, pz = nx + x, ny + y, nz + z
+                                if px < X and py < Y and pz < Z:
+                                    v = np.float32(vox[pz, py, px])
+                                    nlo, nhi = fmin(nlo, v), fmax(nhi, v)
+                if not np.isnan(nlo):
+                    lo = fmin(lo, nlo)
+                if not np.isnan(nhi):
+                    hi = fmax(hi, nhi)
+    return lo, hi
+
+
+@pytest.mark.parametrize("background", [float("nan"), -0.0, 0.5])
+def test_leaf_ranges_follow_reference_fold_order(oracle, background):
+    """The oracle's dense leaf ranges (the parity target of the GPU commit)
+    equal the reference's fold order bit for bit on a volume with NaN and
+    -0.0 voxels, where the order decides the result."""
+    rng = np.random.default_rng(17)
+    dims = (19, 17, 13)
+    vox = rng.uniform(-1, 1, dims[::-1]).astype(np.float32)
+    flat = vox.reshape(-1)
+    flat[rng.choice(flat.size, flat.size // 40, replace=False)] = np.nan
+    flat[rng.choice(flat.size, flat.size // 20, replace=False)] = -0.0
+    flat[rng.choice(flat.size, flat.size // 20, replace=False)] = 0.0
+    vox[4:9] = np.where(rng.random(vox[4:9].shape) < 0.5, np.float32(0.0), np.float32(-0.0))
+    ref = oracle.OracleVolume.dense_volume(vox, background=[background])
+    v2, rng2, _ = ref.level(2, 1)
+    leaf = (v2 & 3) == 3
+    got = rng2[leaf]
+    # one level-2 node; its voxels index leaves as x * 256 + y * 16 + z
+    want = []
+    for lx in range((dims[0] + 7) // 8):
+        for ly in range((dims[1] + 7) // 8):
+            for lz in range((dims[2] + 7) // 8):
+                want.append(_reference_fold_leaf_range(vox, 8 * lx, 8 * ly, 8 * lz, background))
+    want = np.array(want, np.float32)
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
