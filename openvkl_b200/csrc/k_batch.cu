@@ -65,7 +65,9 @@ __device__ __forceinline__ void sampleGradLinear(const Field &F, f3 p, float &v,
   gi.z = lerpf(dx, lerpf(dy, s[1] - s[0], s[3] - s[2]), lerpf(dy, s[5] - s[4], s[7] - s[6]));
 }
 
-template <typename T, bool DENSE, int TILE, bool SORT>
+// ATLAS: dense float jobs whose attribute has a texture atlas fetch their
+// corners from it (AtlasField), as vklComputeSampleN does.
+template <typename T, bool DENSE, int TILE, bool SORT, bool ATLAS = false>
 __global__ void __launch_bounds__(kBatchThreads)
     kBatchLinear(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ tileJob,
                  const uint32_t *__restrict__ jobFirstTile, uint32_t numTiles,
@@ -162,9 +164,12 @@ __global__ void __launch_bounds__(kBatchThreads)
       }
       __syncthreads();
     }
-    using Field = typename std::conditional<DENSE, DenseField<T>, SparseField<T>>::type;
+    using Field = typename std::conditional<
+        ATLAS, AtlasField, typename std::conditional<DENSE, DenseField<T>, SparseField<T>>::type>::type;
     const Field F = [&]() {
-      if constexpr (DENSE)
+      if constexpr (ATLAS)
+        return AtlasField(g, job.attr);
+      else if constexpr (DENSE)
         return DenseField<T>(g, job.attr);
       else
         return SparseField<T>(g, job.attr, kNumLevels - 1);
@@ -215,18 +220,19 @@ enum ClassId : int {
   kDenseU16,
   kDenseF16,
   kDenseF32,
+  kDenseF32Atlas,
   kDenseF64,
   kSparseF32,
   kSparseF16,
   kNumClasses
 };
 
-template <typename T, bool DENSE>
+template <typename T, bool DENSE, bool ATLAS = false>
 Kernel kernelFor(const Config &c)
 {
   if (c.tile == 512)
-    return c.sort ? kBatchLinear<T, DENSE, 512, true> : kBatchLinear<T, DENSE, 512, false>;
-  return c.sort ? kBatchLinear<T, DENSE, 1024, true> : kBatchLinear<T, DENSE, 1024, false>;
+    return c.sort ? kBatchLinear<T, DENSE, 512, true, ATLAS> : kBatchLinear<T, DENSE, 512, false, ATLAS>;
+  return c.sort ? kBatchLinear<T, DENSE, 1024, true, ATLAS> : kBatchLinear<T, DENSE, 1024, false, ATLAS>;
 }
 
 Kernel classKernel(int cls, const Config &c)
@@ -246,18 +252,23 @@ Kernel classKernel(int cls, const Config &c)
     return kernelFor<float, false>(c);
   case kSparseF16:
     return kernelFor<__half, false>(c);
+  case kDenseF32Atlas:
+    return kernelFor<float, true, true>(c);
   default:
     return kernelFor<float, true>(c);
   }
 }
 
-int classOf(const Sampler *s, bool wantGrad)
+// The class of a job on attribute `attr` (its voxel type decides).
+int classOf(const Sampler *s, bool wantGrad, uint32_t attr)
 {
   const DevGrid &g = s->volume->grid;
   if (s->s.filter != kFilterLinear || (wantGrad && s->s.gradientFilter != kFilterLinear))
     return -1;
   if (g.dense) {
-    switch (g.type[0]) {
+    if (g.type[attr] == kFloat && g.atlasTex[attr])
+      return kDenseF32Atlas;
+    switch (g.type[attr]) {
     case kUChar:
       return kDenseU8;
     case kShort:
@@ -274,7 +285,7 @@ int classOf(const Sampler *s, bool wantGrad)
   }
   if (g.compress != kCompressNone || s->s.maxSamplingDepth < kNumLevels - 1)
     return -1;
-  return g.type[0] == kHalf ? kSparseF16 : kSparseF32;
+  return g.type[attr] == kHalf ? kSparseF16 : kSparseF32;
 }
 
 struct ClassPlan {
@@ -528,7 +539,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLCudaSampleBatch vklCudaNewSampleBatch(VKLDe
       grids[i] = s->volume->grid;
       if (jb.numPoints == 0 || (!jb.samples && !jb.gradients))
         continue;
-      const int cls = classOf(s, jb.gradients != nullptr);
+      const int cls = classOf(s, jb.gradients != nullptr, jb.attributeIndex);
       if (cls < 0)
         b->plainJobs.push_back(i);
       else

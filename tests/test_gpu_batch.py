@@ -105,3 +105,30 @@ def test_batch_rejects_host_memory_and_bad_attributes(vkl, device):
     with pytest.raises(vkl.VKLError) as e:
         vkl.SampleBatch(device, [(smp, pts, out, None, 3)])
     assert e.value.code == 2 and "attribute" in e.value.msg
+
+
+def test_batch_jobs_on_mixed_type_attributes(vkl, device):
+    """A job's fused class follows the voxel type of the attribute it samples:
+    jobs on the float (texture atlas), half and int16 attributes of one
+    multi-attribute volume equal the per-call samples and gradients."""
+    import torch
+    dims = (37, 29, 23)
+    f = sinusoid_field(dims, seed=51)
+    attrs = [f, sinusoid_field(dims, seed=52).astype(np.float16),
+             np.clip(sinusoid_field(dims, seed=53) * 40, -32768, 32767).astype(np.int16)]
+    vol = vkl.structured_regular(device, attrs)
+    smp = vkl.Sampler(vol)
+    rng = np.random.default_rng(54)
+    jobs, refs = [], []
+    for attr in (2, 0, 1, 0):
+        pts = torch.from_numpy((rng.random((3000, 3)) * (np.array(dims) + 2) - 1.5).astype(np.float32)).cuda()
+        s = torch.full((3000,), 7.0, device="cuda")
+        g = torch.full((3000, 3), 7.0, device="cuda")
+        jobs.append((smp, pts, s, g, attr))
+        refs.append((smp.sample(pts, attr=attr).cpu().numpy(), smp.gradient(pts, attr=attr).cpu().numpy()))
+    batch = vkl.SampleBatch(device, jobs)
+    assert batch.config()["fused_jobs"] == 4
+    batch.run()
+    torch.cuda.synchronize()
+    _check([j[:4] for j in jobs], refs)
+    batch.release()
