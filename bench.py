@@ -1002,7 +1002,10 @@ def run_commit(args):
                          "frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg, "traffic": None,
                          "note": "whole commit (several kernels, allocations and one readback)"},
-            "cpu_baseline": base, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
+            "cpu_baseline": base, "e2e": e2e,
+            # per commit: kDenseLevel2/1/0, kDenseBrickRanges, kFillEmpty x3,
+            # kLeafToParent, kReduceNodes x2, kVolumeRange (ncu launch list)
+            "gpu_launches": 11 * args.steps, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
