@@ -350,7 +350,7 @@ OPENVKL_CUDA_INTERFACE void vklCudaReleaseSampleBatch(VKLCudaSampleBatch batch);
 // features per level, resolution floor(baseResolution * growth^level) over
 // the volume's object bounding box) feeds a 32-64-64-64-1 ReLU MLP (FP16
 // weights, tensor cores).  The sampler must be trilinear over float voxels;
-// its plain samples are the training targets, the fallback and the judge of
+// its plain samples are the training targets, the fallback and the measure of
 // the surrogate's error.  Parameters (host or device memory): the table as
 // levels x entries x 2 floats, the weights as W1 (64x32), W2 (64x64),
 // W3 (64x64), W4 (64), row-major, concatenated (10304 floats).  Points,

@@ -8,7 +8,7 @@
 // plain sampler (the caller supplies points and the plain samples as
 // targets), with the loss sum (y - target)^2 / n over the points with a
 // finite target, and Adam.  The plain sampler
-// is also the judge: calibration evaluates both on caller-supplied points
+// also measures the error: calibration evaluates both on caller-supplied points
 // and flags every 32^3-voxel region whose largest error exceeds a threshold
 // (or that no calibration point reached); sampling with fallback returns the
 // plain sample there and outside the volume's domain.
