@@ -58,27 +58,8 @@ TRAIN_STEPS = 1024
 # ---------------------------------------------------------------------------
 def volume_numpy(dims=None, seed=1):
     """Seeded sinusoid field, generated slab by slab in float32 (x fastest)."""
-    from openvkl_b200.fields import _sinusoid_params
-    X, Y, Z = dims or DIMS
-    freq, amp, phase = _sinusoid_params(seed)
-    rng = np.random.default_rng(seed + 1000)
-    out = np.empty((Z, Y, X), np.float32)
-    x = (np.arange(X, dtype=np.float32) / X)[None, :]
-    y = (np.arange(Y, dtype=np.float32) / Y)[:, None]
-    two_pi = np.float32(2 * math.pi)
-    # sin(a + c) with a = 2pi(fx x + fy y) + phase per term, c = 2pi fz z
-    sa, ca = [], []
-    for k in range(4):
-        a = two_pi * (np.float32(freq[k, 0]) * x + np.float32(freq[k, 1]) * y) + np.float32(phase[k])
-        sa.append(np.sin(a).astype(np.float32))
-        ca.append(np.cos(a).astype(np.float32))
-    for zi in range(Z):
-        acc = rng.uniform(-0.05, 0.05, size=(Y, X)).astype(np.float32)
-        for k in range(4):
-            c = 2 * math.pi * freq[k, 2] * zi / Z
-            acc += np.float32(amp[k]) * (sa[k] * np.float32(math.cos(c)) + ca[k] * np.float32(math.sin(c)))
-        out[zi] = acc
-    return out
+    from openvkl_b200.fields import sinusoid_volume
+    return sinusoid_volume(dims or DIMS, seed)
 
 
 def points_torch(workload, dims=None, device="cuda"):

@@ -46,6 +46,33 @@ def sinusoid_field(dims, seed=1, noise=0.05, dtype=np.float32):
     return f.astype(dtype)
 
 
+def sinusoid_volume(dims, seed=1):
+    """The sinusoid field of `sinusoid_field` for large volumes: generated
+    z-slab by z-slab in float32 (sin(a + c) expanded per slab), so a 1024^3
+    volume needs no float64 temporaries of its own size.  (Z, Y, X), x
+    fastest; dims = (X, Y, Z)."""
+    X, Y, Z = dims
+    freq, amp, phase = _sinusoid_params(seed)
+    rng = np.random.default_rng(seed + 1000)
+    out = np.empty((Z, Y, X), np.float32)
+    x = (np.arange(X, dtype=np.float32) / X)[None, :]
+    y = (np.arange(Y, dtype=np.float32) / Y)[:, None]
+    two_pi = np.float32(2 * math.pi)
+    # sin(a + c) with a = 2pi(fx x + fy y) + phase per term, c = 2pi fz z
+    sa, ca = [], []
+    for k in range(4):
+        a = two_pi * (np.float32(freq[k, 0]) * x + np.float32(freq[k, 1]) * y) + np.float32(phase[k])
+        sa.append(np.sin(a).astype(np.float32))
+        ca.append(np.cos(a).astype(np.float32))
+    for zi in range(Z):
+        acc = rng.uniform(-0.05, 0.05, size=(Y, X)).astype(np.float32)
+        for k in range(4):
+            c = 2 * math.pi * freq[k, 2] * zi / Z
+            acc += np.float32(amp[k]) * (sa[k] * np.float32(math.cos(c)) + ca[k] * np.float32(math.sin(c)))
+        out[zi] = acc
+    return out
+
+
 def sinusoid_field_torch(dims, seed=1, noise=0.05, device="cuda"):
     """Same distribution as sinusoid_field, generated on the GPU in slabs of
     about 2^24 voxels."""

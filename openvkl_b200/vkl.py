@@ -640,11 +640,12 @@ class Surrogate:
 
 def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, packed_tile=None,
                node_data=None, index_to_object=None, index_clipping_bounds=None, background=None,
-               compression=None, leaf_map=None):
+               compression=None, leaf_map=None, shared=False):
     """A committed vdb volume from packed leaves (nodesPackedDense / Tile, one
     array or a list per attribute) or per-leaf node.data arrays.
     `compression` ("fp16" | "bf16" | "fp8") stores float leaves as codes with
-    a per-leaf scale and offset (cuda device extension)."""
+    a per-leaf scale and offset (cuda device extension).  `shared`: the
+    packed leaf arrays are VKL_DATA_SHARED_BUFFER (used in place)."""
     v = Volume(device, "vdb")
     v.set_data("node.level", Data(device, np.ascontiguousarray(levels, np.uint32)))
     v.set_data("node.origin", Data(device, np.ascontiguousarray(origins, np.int32).reshape(-1),
@@ -652,7 +653,7 @@ def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, pack
     v.set_data("node.format", Data(device, np.ascontiguousarray(formats, np.uint32)))
     if packed_dense is not None:
         pd = packed_dense if isinstance(packed_dense, (list, tuple)) else [packed_dense]
-        v.set_data("nodesPackedDense", Data(device, objects=[Data(device, a) for a in pd]))
+        v.set_data("nodesPackedDense", Data(device, objects=[Data(device, a, shared=shared) for a in pd]))
         if packed_tile is not None:
             pt = packed_tile if isinstance(packed_tile, (list, tuple)) else [packed_tile]
             v.set_data("nodesPackedTile", Data(device, objects=[Data(device, a) for a in pt]))
@@ -774,7 +775,11 @@ class Sampler(_Obj):
 
 
 class IntervalIteratorContext(_Obj):
-    def __init__(self, sampler: Sampler, value_ranges=None, hint=None, attr=None):
+    """vklNewIntervalIteratorContext.  `macrocells`: intervals of 16^3-voxel
+    macrocells, the iterator of the reference's legacy structuredRegular
+    volume (cuda device extension; vklIterateIntervalsN only)."""
+
+    def __init__(self, sampler: Sampler, value_ranges=None, hint=None, attr=None, macrocells=False):
         super().__init__(sampler.device, sampler.lib.vklNewIntervalIteratorContext(sampler.h))
         self._check_handle("vklNewIntervalIteratorContext")
         self.sampler = sampler
@@ -785,6 +790,8 @@ class IntervalIteratorContext(_Obj):
             self.set_float("intervalResolutionHint", hint)
         if attr is not None:
             self.set_int("attributeIndex", attr)
+        if macrocells:
+            self.set_bool("macrocells", True)
         self.commit()
 
     def iterate_n(self, origins, directions, t_ranges, max_per_ray=64):

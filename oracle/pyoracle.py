@@ -45,10 +45,13 @@ def fast_path() -> str:
     return os.path.join(_BUILD, f"liboracle_fast_{_host_tag()}.so")
 
 
-def build(fast: bool = True) -> None:
+def build(fast: bool = True, fma: bool = False) -> None:
     """Compile the parity build with the committed Makefile and, if asked,
-    the -march=native timing build for this host."""
+    the -march=native timing build for this host and the FP-contraction
+    build."""
     subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle.so"], check=True)
+    if fma:
+        subprocess.run(["make", "-s", "-C", _HERE, "build/liboracle_fma.so"], check=True)
     srcs = [os.path.join(_HERE, f) for f in ("vkl_oracle.cpp", "vkl_oracle.h")]
     stale = not os.path.exists(fast_path()) or \
         os.path.getmtime(fast_path()) < max(os.path.getmtime(f) for f in srcs)
@@ -60,11 +63,14 @@ def build(fast: bool = True) -> None:
 _libs: dict = {}
 
 
-def lib(fast: bool = False) -> C.CDLL:
-    name = fast_path() if fast else os.path.join(_BUILD, "liboracle.so")
+def lib(fast: bool = False, fma: bool = False) -> C.CDLL:
+    """The parity build; `fast`: the -march=native timing build; `fma`: the
+    build whose float expressions are contracted into FMAs."""
+    name = os.path.join(_BUILD, "liboracle_fma.so") if fma else (
+        fast_path() if fast else os.path.join(_BUILD, "liboracle.so"))
     if name not in _libs:
         path = name
-        build(fast=fast)
+        build(fast=fast, fma=fma)
         L = C.CDLL(path)
         P, U32, U64, I32, F32, VP = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float, C.c_void_p
         L.orc_dense_create.restype = P
@@ -81,6 +87,10 @@ def lib(fast: bool = False) -> C.CDLL:
         L.orc_sample.argtypes = [P, C.c_int, U32, U64, P, U32, P]
         L.orc_gradient.argtypes = [P, C.c_int, U32, U64, P, U32, P]
         L.orc_sample_parallel.argtypes = [P, C.c_int, U64, P, U32, P, C.c_int]
+        L.orc_gradient_parallel.argtypes = [P, C.c_int, U32, U64, P, U32, P, C.c_int]
+        L.orc_macrocell_ranges.argtypes = [P, U32, P]
+        L.orc_iterate_macrocells.restype = C.c_int
+        L.orc_iterate_macrocells.argtypes = [P, U32, U32, P, U64, P, P, P, U32, P, P]
         L.orc_sample_observed.argtypes = [P, C.c_int, U32, U64, P, U32, P, P]
         L.orc_sample_fp64.argtypes = [P, C.c_int, U64, P, U32, P]
         L.orc_iterate_intervals.argtypes = [P, U32, U32, P, F32, U64, P, P, P, U32, P, P]
@@ -104,10 +114,10 @@ def _p(a):
 class OracleVolume:
     """A committed oracle volume (dense structuredRegular or sparse VDB)."""
 
-    def __init__(self, handle, keep, fast=False):
+    def __init__(self, handle, keep, fast=False, fma=False):
         self._h = handle
         self._keep = keep  # numpy buffers the oracle points into
-        self._lib = lib(fast)
+        self._lib = lib(fast, fma)
         info = self.info()
         self.dense = keep.get("dense", False)
         self.o2i, self.i2o = info["o2i"], info["i2o"]
@@ -122,7 +132,7 @@ class OracleVolume:
     # ---- construction -------------------------------------------------
     @staticmethod
     def dense_volume(data, cell_centered=False, grid_origin=None, grid_spacing=None,
-                     index_to_object=None, index_origin=None, background=None, fast=False):
+                     index_to_object=None, index_origin=None, background=None, fast=False, fma=False):
         """`data`: one array (or a list of arrays, one per attribute) shaped
         (Z, Y, X) so that x is fastest in memory."""
         arrays = data if isinstance(data, (list, tuple)) else [data]
@@ -136,16 +146,17 @@ class OracleVolume:
         i2o = None if index_to_object is None else np.asarray(index_to_object, np.float32)
         io = None if index_origin is None else np.asarray(index_origin, np.int32)
         bg = None if background is None else np.asarray(background, np.float32).reshape(-1)
-        L = lib(fast)
+        L = lib(fast, fma)
         h = L.orc_dense_create(_p(dims), len(arrays), ptrs, _p(types), _p(strides),
                                int(bool(cell_centered)), _p(go), _p(gs), _p(i2o), _p(io), _p(bg))
         if not h:
             raise RuntimeError(L.orc_last_error().decode())
-        return OracleVolume(h, {"arrays": arrays, "dense": True}, fast)
+        return OracleVolume(h, {"arrays": arrays, "dense": True}, fast, fma)
 
     @staticmethod
     def vdb_volume(levels, origins, formats, packed_dense, packed_tile=None,
-                   index_to_object=None, index_clipping_bounds=None, background=None, fast=False):
+                   index_to_object=None, index_clipping_bounds=None, background=None, fast=False,
+                   fma=False):
         levels = np.ascontiguousarray(levels, np.uint32)
         origins = np.ascontiguousarray(origins, np.int32).reshape(-1, 3)
         formats = np.ascontiguousarray(formats, np.uint32)
@@ -162,12 +173,12 @@ class OracleVolume:
         i2o = None if index_to_object is None else np.asarray(index_to_object, np.float32)
         clip = None if index_clipping_bounds is None else np.asarray(index_clipping_bounds, np.int32)
         bg = None if background is None else np.asarray(background, np.float32).reshape(-1)
-        L = lib(fast)
+        L = lib(fast, fma)
         h = L.orc_vdb_create(len(levels), _p(levels), _p(origins), _p(formats), len(pd), dtype,
                              pdp, ptp, _p(i2o), _p(clip), _p(bg))
         if not h:
             raise RuntimeError(L.orc_last_error().decode())
-        return OracleVolume(h, {"pd": pd, "pt": pt, "dense": False}, fast)
+        return OracleVolume(h, {"pd": pd, "pt": pt, "dense": False}, fast, fma)
 
     # ---- introspection ------------------------------------------------
     def info(self):
@@ -225,6 +236,13 @@ class OracleVolume:
         self._lib.orc_gradient(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out))
         return out
 
+    def gradient_parallel(self, points, filter=FILTER_LINEAR, attr=0, max_sampling_depth=3, threads=0):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros((len(pts), 3), np.float32)
+        self._lib.orc_gradient_parallel(self._h, filter, max_sampling_depth, len(pts), _p(pts), attr, _p(out),
+                                        threads)
+        return out
+
     def sample_fp64(self, points, filter=FILTER_LINEAR, attr=0):
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         out = np.zeros(len(pts), np.float64)
@@ -243,6 +261,28 @@ class OracleVolume:
         cnt = np.zeros(len(o), np.uint32)
         self._lib.orc_iterate_intervals(self._h, attr, nvr, _p(vr), hint, len(o), _p(o), _p(d),
                                         _p(t), max_intervals, _p(out), _p(cnt))
+        return out, cnt
+
+    def macrocell_ranges(self, attr=0):
+        """(nz, ny, nx, 2) value ranges of the 16^3-voxel macrocells."""
+        d = self._keep["arrays"][0].shape  # (Z, Y, X)
+        n = [((x - 1) >> 4) + 1 for x in d]
+        out = np.zeros((n[0], n[1], n[2], 2), np.float32)
+        self._lib.orc_macrocell_ranges(self._h, attr, _p(out))
+        return out
+
+    def macrocell_intervals(self, origins, directions, t_ranges, value_ranges=None, attr=0, max_intervals=64):
+        """Intervals of the legacy 16^3 macrocell iterator: ((n, max, 5), counts)."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(t_ranges, np.float32).reshape(-1, 2)
+        vr = None if value_ranges is None else np.ascontiguousarray(value_ranges, np.float32).reshape(-1, 2)
+        nvr = 0 if vr is None else len(vr)
+        out = np.zeros((len(o), max_intervals, 5), np.float32)
+        cnt = np.zeros(len(o), np.uint32)
+        if self._lib.orc_iterate_macrocells(self._h, attr, nvr, _p(vr), len(o), _p(o), _p(d), _p(t),
+                                            max_intervals, _p(out), _p(cnt)):
+            raise RuntimeError(self._lib.orc_last_error().decode())
         return out, cnt
 
     def hits(self, origins, directions, t_ranges, values, filter=FILTER_LINEAR, attr=0, max_hits=16):

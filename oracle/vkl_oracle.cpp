@@ -122,6 +122,13 @@ struct range1f {
 inline float fmin_(float a, float b) { return a < b ? a : b; }
 inline float fmax_(float a, float b) { return a > b ? a : b; }
 
+// float -> int32 truncation as x86 cvttss2si does it (ISPC to_int): NaN and
+// out-of-range values give INT32_MIN.
+inline int32_t toIntX86(float x)
+{
+  return (x >= -2147483648.f && x < 2147483648.f) ? (int32_t)x : INT32_MIN;
+}
+
 // rkcommon lerp(factor, a, b) = (1 - factor) * a + factor * b (the form used
 // by rkcommon/math; not vendored in the reference tree, so parity-unpinned).
 inline float lerp(float f, float a, float b) { return (1.f - f) * a + f * b; }
@@ -245,6 +252,10 @@ struct Grid {
   std::vector<float> background;
   // dense
   vec3i denseDims;
+  // gridOrigin / gridSpacing of a vertex-centered dense volume without
+  // indexToObject or indexOrigin (what the legacy macrocell iterator reads)
+  bool legacyGrid = false;
+  float gridOrigin[3] = {0, 0, 0}, gridSpacing[3] = {1, 1, 1};
   std::vector<Attr> denseAttr;
   std::vector<std::vector<uint8_t>> denseCopies;
   // sparse packed
@@ -1378,6 +1389,12 @@ OrcVolume *orc_dense_create(const int32_t dims[3], uint32_t numAttributes,
                            gridSpacing ? gridSpacing[2] : 1.f};
       const float cc[12] = {gs[0], 0, 0, 0, gs[1], 0, 0, 0, gs[2], go[0], go[1], go[2]};
       std::memcpy(c, cc, sizeof(c));
+      for (int a = 0; a < 3; ++a) {
+        g.gridOrigin[a]  = go[a];
+        g.gridSpacing[a] = gs[a];
+      }
+      g.legacyGrid = !cellCentered &&
+                     (!indexOrigin || (indexOrigin[0] == 0 && indexOrigin[1] == 0 && indexOrigin[2] == 0));
     }
     makeTransforms(c, g.i2o, g.o2i);
     const vec3i io = {indexOrigin ? indexOrigin[0] : 0, indexOrigin ? indexOrigin[1] : 0,
@@ -1590,6 +1607,17 @@ void orc_gradient(const OrcVolume *v, int filter, uint32_t depth, uint64_t n, co
   }
 }
 
+void orc_gradient_parallel(const OrcVolume *v, int filter, uint32_t depth, uint64_t n,
+                           const float *pts, uint32_t attr, float *out, int threads)
+{
+  // orc_gradient over chunks of 4096 points on `threads` host threads
+  const uint64_t chunks = (n + 4095) / 4096;
+  parallelFor((int64_t)chunks, threads, 1, [&](int64_t c) {
+    const uint64_t b = (uint64_t)c * 4096, e = std::min<uint64_t>(n, b + 4096);
+    orc_gradient(v, filter, depth, e - b, pts + 3 * b, attr, out + 3 * b);
+  });
+}
+
 void orc_sample_fp64(const OrcVolume *v, int filter, uint64_t n, const float *pts,
                      uint32_t attr, double *out)
 {
@@ -1687,6 +1715,196 @@ void orc_iterate_intervals(const OrcVolume *v, uint32_t attr, uint32_t numRanges
     }
     counts[r] = c;
   });
+}
+
+// ---------------------------------------------------------------------------
+// 16^3-voxel macrocell intervals: the iterator of the reference's legacy
+// structuredRegular volume (the GridAccelerator, built when
+// OPENVKL_DEVICE_CPU_STRUCTURED_REGULAR_LEGACY is on).  Macrocell width
+// GridAccelerator.h:14-19; macrocell value ranges GridAccelerator.ispc:80-109
+// (vertices cell*16 + [0, 16] per axis, clamped to dims - 1, NaN skipped, NaN
+// range if all are NaN; SharedStructuredVolume.ispc:196-209 for a vertex's
+// range); cell walk GridAccelerator_nextCell, GridAccelerator.ispc:146-240;
+// interval emission GridAcceleratorIterator.ispc:44-155.  Transforms
+// SharedStructuredVolume.ih:21-53, bounding box StructuredVolume.cpp:205-211.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int MACRO_BITS = 4;  // CELL_WIDTH_BITCOUNT
+
+inline vec3i macrocellCount(const Grid &g)
+{
+  return {((g.denseDims.x - 1) >> MACRO_BITS) + 1, ((g.denseDims.y - 1) >> MACRO_BITS) + 1,
+          ((g.denseDims.z - 1) >> MACRO_BITS) + 1};
+}
+
+range1f macrocellRange(const Grid &g, uint32_t a, int cx, int cy, int cz)
+{
+  range1f r;
+  bool empty = true;
+  const vec3i d = g.denseDims;
+  for (int k = 0; k <= (1 << MACRO_BITS); ++k)
+    for (int j = 0; j <= (1 << MACRO_BITS); ++j)
+      for (int i = 0; i <= (1 << MACRO_BITS); ++i) {
+        const int x = std::min(d.x - 1, (cx << MACRO_BITS) + i), y = std::min(d.y - 1, (cy << MACRO_BITS) + j),
+                  z = std::min(d.z - 1, (cz << MACRO_BITS) + k);
+        const float v = loadAttr(g.denseAttr[a], (uint64_t)x + (uint64_t)d.x * ((uint64_t)y + (uint64_t)d.y * (uint64_t)z));
+        if (!std::isnan(v)) {
+          r.lower = fmin_(r.lower, v);
+          r.upper = fmax_(r.upper, v);
+          empty   = false;
+        }
+      }
+  if (empty)
+    r.lower = r.upper = std::numeric_limits<float>::quiet_NaN();
+  return r;
+}
+
+struct MacroIt {
+  vec3f o, d;
+  range1f bbT;
+  vec3i cell;
+  float nominalDeltaT;
+};
+
+inline vec3f toLocal(const Grid &g, const vec3f &p)
+{
+  return {1.f / g.gridSpacing[0] * (p.x - g.gridOrigin[0]), 1.f / g.gridSpacing[1] * (p.y - g.gridOrigin[1]),
+          1.f / g.gridSpacing[2] * (p.z - g.gridOrigin[2])};
+}
+
+inline range1f macrocellT(const Grid &g, const MacroIt &it, const vec3i &c)
+{
+  // GridAccelerator_getCellBounds: lower/upper corner of the cell in object space
+  float box[6];
+  const int lo[3] = {c.x << MACRO_BITS, c.y << MACRO_BITS, c.z << MACRO_BITS};
+  const int hi[3] = {(c.x + 1) << MACRO_BITS, (c.y + 1) << MACRO_BITS, (c.z + 1) << MACRO_BITS};
+  for (int a = 0; a < 3; ++a) {
+    box[a]     = g.gridOrigin[a] + (float)lo[a] * g.gridSpacing[a];
+    box[3 + a] = g.gridOrigin[a] + (float)hi[a] * g.gridSpacing[a];
+  }
+  return intersectBox(it.o, it.d, box, it.bbT);
+}
+
+// isempty1f (math/box_utility.ih:6-9)
+inline bool isEmpty1f(const range1f &r) { return r.upper <= r.lower; }
+
+bool macroNextCell(const Grid &g, MacroIt &it, range1f &cellT)
+{
+  const bool first = it.cell.x == -1;
+  range1f iv;
+  if (first) {
+    const vec3f p  = {it.o.x + it.bbT.lower * it.d.x, it.o.y + it.bbT.lower * it.d.y, it.o.z + it.bbT.lower * it.d.z};
+    const vec3f lc = toLocal(g, p);
+    it.cell        = {toIntX86(lc.x) >> MACRO_BITS, toIntX86(lc.y) >> MACRO_BITS, toIntX86(lc.z) >> MACRO_BITS};
+    iv             = macrocellT(g, it, it.cell);
+  }
+  if (!first || isEmpty1f(iv)) {
+    // direction * 1.f / gridSpacing * RCP_CELL_WIDTH, RCP_CELL_WIDTH being the
+    // macro text "1.f / CELL_WIDTH": ((d * 1) / s * 1) / 16
+    const float cd[3]  = {it.d.x / g.gridSpacing[0] / 16.f, it.d.y / g.gridSpacing[1] / 16.f,
+                          it.d.z / g.gridSpacing[2] / 16.f};
+    const float rcd[3] = {rcp_safe(cd[0]), rcp_safe(cd[1]), rcp_safe(cd[2])};
+    const vec3f lo     = toLocal(g, it.o);
+    const float co[3]  = {lo.x / 16.f, lo.y / 16.f, lo.z / 16.f};
+    int corner[3];
+    float tMax[3];
+    const int ci[3] = {it.cell.x, it.cell.y, it.cell.z};
+    for (int a = 0; a < 3; ++a) {
+      uint32_t bits;
+      std::memcpy(&bits, &cd[a], 4);
+      corner[a]      = 1 - 2 * (int)(bits >> 31);
+      const float t0 = ((float)ci[a] - co[a]) * rcd[a];
+      const float t1 = ((float)(ci[a] + 1) - co[a]) * rcd[a];
+      tMax[a]        = fmax_(t0, t1);
+    }
+    const float tExit = fmin_(fmin_(tMax[0], tMax[1]), tMax[2]);
+    it.cell = {ci[0] + (tMax[0] == tExit ? corner[0] : 0), ci[1] + (tMax[1] == tExit ? corner[1] : 0),
+               ci[2] + (tMax[2] == tExit ? corner[2] : 0)};
+    iv      = macrocellT(g, it, it.cell);
+  }
+  if (isEmpty1f(iv)) {
+    cellT = range1f();
+    return false;
+  }
+  cellT = iv;
+  return true;
+}
+
+}  // namespace
+
+void orc_macrocell_ranges(const OrcVolume *v, uint32_t attr, float *out)
+{
+  const Grid &g = v->g;
+  const vec3i n = macrocellCount(g);
+  parallelFor((int64_t)n.x * n.y * n.z, 0, 64, [&](int64_t c) {
+    const int cx = (int)(c % n.x), cy = (int)((c / n.x) % n.y), cz = (int)(c / ((int64_t)n.x * n.y));
+    const range1f r = macrocellRange(g, attr, cx, cy, cz);
+    out[2 * c]      = r.lower;
+    out[2 * c + 1]  = r.upper;
+  });
+}
+
+int orc_iterate_macrocells(const OrcVolume *v, uint32_t attr, uint32_t numRanges, const float *ranges,
+                           uint64_t numRays, const float *origins, const float *directions,
+                           const float *tRanges, uint32_t maxIntervals, float *out, uint32_t *counts)
+{
+  const Grid &g = v->g;
+  if (!g.dense || !g.legacyGrid) {
+    g_lastError = "macrocell intervals need a vertex-centered structuredRegular volume given by "
+                  "gridOrigin / gridSpacing";
+    return 1;
+  }
+  ValueRanges vr;
+  for (uint32_t i = 0; i < numRanges; ++i)
+    vr.ranges.push_back({ranges[2 * i], ranges[2 * i + 1]});
+  vr.computeMinMax();
+  const vec3i n = macrocellCount(g);
+  std::vector<range1f> cr((size_t)n.x * n.y * n.z);
+  parallelFor((int64_t)cr.size(), 0, 64, [&](int64_t c) {
+    cr[c] = macrocellRange(g, attr, (int)(c % n.x), (int)((c / n.x) % n.y), (int)(c / ((int64_t)n.x * n.y)));
+  });
+  float box[6];
+  for (int a = 0; a < 3; ++a) {
+    const int d = a == 0 ? g.denseDims.x : a == 1 ? g.denseDims.y : g.denseDims.z;
+    box[a]      = g.gridOrigin[a];
+    box[3 + a]  = g.gridOrigin[a] + (float)(d - 1) * g.gridSpacing[a];
+  }
+  parallelFor((int64_t)numRays, 0, 64, [&](int64_t r) {
+    MacroIt it;
+    it.o   = {origins[3 * r], origins[3 * r + 1], origins[3 * r + 2]};
+    it.d   = {directions[3 * r], directions[3 * r + 1], directions[3 * r + 2]};
+    it.bbT = intersectBox(it.o, it.d, box, {tRanges[2 * r], tRanges[2 * r + 1]});
+    it.cell = {-1, -1, -1};
+    it.nominalDeltaT = fmin_(fmin_(g.gridSpacing[0] * rcp_safe(std::fabs(it.d.x)),
+                                   g.gridSpacing[1] * rcp_safe(std::fabs(it.d.y))),
+                             g.gridSpacing[2] * rcp_safe(std::fabs(it.d.z)));
+    uint32_t c = 0;
+    if (!isEmpty1f(it.bbT)) {
+      range1f t;
+      int budget = 4 * (n.x + n.y + n.z) + 16;
+      while (budget-- > 0 && macroNextCell(g, it, t)) {
+        // the cell's stored range (cells the walk reaches lie in the grid; the
+        // index is clamped for the lookup)
+        const int x = std::min(std::max(it.cell.x, 0), n.x - 1), y = std::min(std::max(it.cell.y, 0), n.y - 1),
+                  z = std::min(std::max(it.cell.z, 0), n.z - 1);
+        const range1f vrng = cr[(size_t)x + (size_t)n.x * ((size_t)y + (size_t)n.y * z)];
+        if (!vr.overlaps(vrng))
+          continue;
+        if (c < maxIntervals) {
+          float *o = out + ((uint64_t)r * maxIntervals + c) * 5;
+          o[0] = t.lower;
+          o[1] = t.upper;
+          o[2] = vrng.lower;
+          o[3] = vrng.upper;
+          o[4] = it.nominalDeltaT;
+        }
+        c++;
+      }
+    }
+    counts[r] = c;
+  });
+  return 0;
 }
 
 namespace {

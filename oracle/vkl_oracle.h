@@ -101,7 +101,8 @@ void orc_gradient(const OrcVolume *v,
 // every leaf a tap's tree walk reaches is set to 1 (VdbLeafAccessObserver.ih).
 void orc_sample_observed(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint64_t n,
                          const float *points, uint32_t attr, float *out, uint32_t *leafAccess);
-// Same as orc_sample but split over `threads` OpenMP threads (CPU baseline).
+// Same as orc_sample but split over `threads` host threads (CPU baseline,
+// and the large parity cases).
 void orc_sample_parallel(const OrcVolume *v,
                          int filter,
                          uint64_t n,
@@ -109,6 +110,18 @@ void orc_sample_parallel(const OrcVolume *v,
                          uint32_t attr,
                          float *out,
                          int threads);
+// 16^3-voxel macrocell intervals of the reference's legacy structuredRegular
+// volume (GridAccelerator): per-macrocell value ranges (2 floats per cell,
+// x fastest) and the batched interval walk (out: maxIntervals x 5 floats per
+// ray, counts: all intervals of the ray).  Returns nonzero (orc_last_error)
+// for volumes the legacy iterator does not cover.
+void orc_macrocell_ranges(const OrcVolume *v, uint32_t attr, float *out);
+int orc_iterate_macrocells(const OrcVolume *v, uint32_t attr, uint32_t numRanges, const float *ranges,
+                           uint64_t numRays, const float *origins, const float *directions,
+                           const float *tRanges, uint32_t maxIntervals, float *out, uint32_t *counts);
+// orc_gradient split over `threads` host threads.
+void orc_gradient_parallel(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint64_t n,
+                           const float *points, uint32_t attr, float *out, int threads);
 
 // FP64 evaluation of the same filter on the stored voxel values (error
 // reporting only).
