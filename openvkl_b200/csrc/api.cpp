@@ -807,6 +807,10 @@ VKLIntervalIterator vklInitIntervalIterator(const VKLIntervalIteratorContext *co
         if (!context || !buffer || !origin || !direction || !tRange)
           fail("vklInitIntervalIterator: NULL argument", VKL_INVALID_ARGUMENT);
         IntervalContext *c = objectAs<IntervalContext>(*context, "interval iterator context");
+        if (c->macrocells)
+          fail("vklInitIntervalIterator: macrocell intervals (context parameter \"macrocells\") are "
+               "produced by vklIterateIntervalsN",
+               VKL_INVALID_OPERATION);
         Device *d          = c->device;
         IterHeader *h      = (IterHeader *)buffer;
         h->magic           = kIntervalMagic;
@@ -953,10 +957,16 @@ void vklIterateIntervalsN(const VKLIntervalIteratorContext *context, unsigned in
     const bool dev = isDevicePtr(origins) && isDevicePtr(directions) && isDevicePtr(tRanges) &&
                      isDevicePtr(counts) && (maxPerRay == 0 || isDevicePtr(intervals));
     const DevGrid &g = c->sampler->volume->grid;
+    const float *macro = c->macrocells ? c->sampler->volume->macrocellRanges(c->attr, d->stream) : nullptr;
+    auto launch = [&](const float *o, const float *dr, const float *t, DevInterval *iv, uint32_t *cnt) {
+      if (macro)
+        launchMacrocellIntervals(g, macro, c->devValueRanges(), N, o, dr, t, maxPerRay, iv, cnt, d->stream);
+      else
+        launchIntervals(g, c->attr, c->depth, c->devValueRanges(), N, o, dr, t, maxPerRay, iv, cnt, d->stream);
+    };
     if (dev) {
-      launchIntervals(g, c->attr, c->depth, c->devValueRanges(), N, (const float *)origins,
-                      (const float *)directions, (const float *)tRanges, maxPerRay,
-                      (DevInterval *)intervals, counts, d->stream);
+      launch((const float *)origins, (const float *)directions, (const float *)tRanges, (DevInterval *)intervals,
+             counts);
       return;
     }
     std::lock_guard<std::mutex> lock(d->stagingMutex);
@@ -971,9 +981,7 @@ void vklIterateIntervalsN(const VKLIntervalIteratorContext *context, unsigned in
               "stage");
     DevInterval *dIv = (DevInterval *)out;
     uint32_t *dCnt   = (uint32_t *)(out + (size_t)N * maxPerRay * 20);
-    launchIntervals(g, c->attr, c->depth, c->devValueRanges(), N, (const float *)in,
-                    (const float *)(in + N * 12), (const float *)(in + N * 24), maxPerRay, dIv,
-                    dCnt, d->stream);
+    launch((const float *)in, (const float *)(in + N * 12), (const float *)(in + N * 24), dIv, dCnt);
     if (maxPerRay)
       cudaCheck(cudaMemcpyAsync(intervals, dIv, (size_t)N * maxPerRay * 20, cudaMemcpyDeviceToHost,
                                 d->stream),

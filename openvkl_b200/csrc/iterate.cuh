@@ -333,8 +333,9 @@ __device__ inline bool intervalNext(const DevGrid &g, uint32_t attr, const DevVa
 // Hit iteration.
 // ---------------------------------------------------------------------------
 // Out of line so the many call sites of the bisection share one copy of the
-// type / filter dispatch.
-__device__ __noinline__ float hitSample(const DevGrid &g, int filter, uint32_t attr, uint32_t depth,
+// type / filter dispatch (static: one copy per translation unit that
+// includes this header).
+static __device__ __noinline__ float hitSample(const DevGrid &g, int filter, uint32_t attr, uint32_t depth,
                                         f3 p)
 {
   return sampleObjectAny(g, filter, attr, depth, p);

@@ -66,6 +66,15 @@ void launchIntervals(const DevGrid &g, uint32_t attr, uint32_t depth, DevValueRa
                      uint64_t n, const float *origins, const float *directions,
                      const float *tRanges, uint32_t maxPerRay, DevInterval *out,
                      uint32_t *counts, cudaStream_t stream);
+// 16^3-voxel macrocell intervals (k_macrocell.cu): the volume check (throws
+// for volumes the legacy iterator does not cover), the number of
+// macrocells, their value ranges (2 floats each) and the batched walk.
+void checkMacrocellVolume(const DevGrid &g);
+uint64_t macrocellRangeCount(const DevGrid &g);
+void launchMacrocellRanges(const DevGrid &g, uint32_t attr, float *ranges, cudaStream_t stream);
+void launchMacrocellIntervals(const DevGrid &g, const float *ranges, DevValueRanges vr, uint64_t n,
+                              const float *origins, const float *directions, const float *tRanges,
+                              uint32_t maxPerRay, DevInterval *out, uint32_t *counts, cudaStream_t stream);
 // Batched hit iteration: one thread per ray.
 void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, DevValueRanges vr,
                 uint32_t numValues, const float *values, uint64_t n, const float *origins,

@@ -475,6 +475,8 @@ void Volume::commit()
   keep.clear();
   committed = false;
   grid      = DevGrid{};
+  for (auto &m : macroRanges)
+    m.reset();
   filter = getInt("filter", VKL_FILTER_LINEAR);
   gradientFilter = getInt("gradientFilter", filter);
   maxSamplingDepth = (uint32_t)std::min(getInt("maxSamplingDepth", (int)kNumLevels - 1),
@@ -1136,6 +1138,11 @@ void IntervalContext::commit()
     ranges.assign(v, v + 2 * d->numItems);
   }
   minMaxOf(ranges, minMax);
+  macrocells = getBool("macrocells", false);
+  if (macrocells) {
+    checkMacrocellVolume(sampler->volume->grid);
+    sampler->volume->macrocellRanges(attr, device->stream);
+  }
   const float hint = getFloat("intervalResolutionHint", 0.5f);
   depth            = hintToDepth(hint);
   elementary       = std::max(std::min(1.f, hint), 0.f) == 1.f;
@@ -1148,6 +1155,17 @@ void IntervalContext::commit()
   if (!devState.ptr)
     devState.alloc(sizeof(state));
   cudaCheck(cudaMemcpy(devState.ptr, &state, sizeof(state), cudaMemcpyHostToDevice), "upload");
+}
+
+const float *Volume::macrocellRanges(uint32_t attr, cudaStream_t st)
+{
+  if (!macroRanges[attr]) {
+    std::unique_ptr<DeviceBuffer> b(new DeviceBuffer());
+    b->alloc(macrocellRangeCount(grid) * 8);
+    launchMacrocellRanges(grid, attr, b->as<float>(), st);
+    macroRanges[attr] = std::move(b);
+  }
+  return macroRanges[attr]->as<float>();
 }
 
 DevValueRanges IntervalContext::devValueRanges() const

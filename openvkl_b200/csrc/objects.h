@@ -304,6 +304,10 @@ struct Volume : ManagedObject {
   const char *typeName() const override { return isDense ? "structuredRegular" : "vdb"; }
   void commit() override;
   ~Volume() override;
+  // Value ranges of the 16^3-voxel macrocells of one attribute (interval
+  // contexts with "macrocells" = 1), built on first use after a commit.
+  std::unique_ptr<DeviceBuffer> macroRanges[kMaxAttributes];
+  const float *macrocellRanges(uint32_t attr, cudaStream_t st);
   std::unique_ptr<TextureAtlas> atlases[kMaxAttributes];
   // Device buffers of the previous commit.  A re-commit takes buffers of
   // the sizes it needs from here (a time-varying volume re-committed with
@@ -353,6 +357,9 @@ struct IntervalContext : ManagedObject {
   float minMax[2]   = {0, 0};
   uint32_t depth    = 2;
   bool elementary   = false;
+  // extension: intervals of 16^3-voxel macrocells (the reference's legacy
+  // structuredRegular iterator) instead of the hierarchy walk
+  bool macrocells = false;
   DeviceBuffer devRanges;
   DeviceBuffer devState;  // DevIntervalContextState for the device-side API
   const char *typeName() const override { return "IntervalIteratorContext"; }

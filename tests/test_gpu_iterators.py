@@ -120,3 +120,45 @@ def test_per_ray_api_equals_batched(vkl, device, oracle):
         h1 = hctx.iterate_one(o[r], d[r], t[r])
         assert len(h1) == hcnt[r]
         np.testing.assert_array_equal(bits(h1), bits(hgot[r, :hcnt[r]]))
+
+
+def test_macrocell_intervals(vkl, device, oracle):
+    """16^3-voxel macrocell intervals (context parameter "macrocells", the
+    interval walk of the reference's legacy structuredRegular volume; an
+    extension here): dims that are not multiples of 16, a grid origin and
+    anisotropic spacing, rays from all sides, with and without value-range
+    filters; counts and intervals bit-exact against the oracle."""
+    dims = (53, 40, 37)
+    vox = sinusoid_field(dims, seed=23)
+    kw = dict(grid_origin=(-3.0, 2.5, 1.0), grid_spacing=(0.5, 1.25, 0.75))
+    ref = oracle.OracleVolume.dense_volume(vox, **kw)
+    vol = vkl.structured_regular(device, vox, **kw)
+    b = ref.info()["bounds"]
+    o, d, t = random_rays(4000, b[:3], b[3:], seed=7)
+    # axis-aligned rays, rays starting inside, and a bounded t range
+    o[:200] = (b[:3] + b[3:]) / 2
+    d[:200] = np.eye(3, dtype=np.float32)[np.arange(200) % 3] * np.where(np.arange(200) % 2, 1, -1)[:, None]
+    t[200:400] = [[5.0, 20.0]]
+    lo, hi = float(vox.min()), float(vox.max())
+    for vr in (None, [[lo, lo + 0.2 * (hi - lo)]], [[lo, lo + 0.1], [hi - 0.3, hi]]):
+        ctx = vkl.IntervalIteratorContext(vkl.Sampler(vol), value_ranges=vr, macrocells=True)
+        got, gcnt = ctx.iterate_n(o, d, t, max_per_ray=32)
+        want, wcnt = ref.macrocell_intervals(o, d, t, value_ranges=vr, max_intervals=32)
+        _compare_intervals(got, gcnt, want, wcnt)
+        assert gcnt.sum() > 0
+
+
+def test_macrocell_intervals_reject_unsupported(vkl, device):
+    """The legacy walk covers vertex-centered volumes given by gridOrigin /
+    gridSpacing: a rotated or cell-centered volume is rejected at the
+    context's commit, and the per-ray API refuses macrocell contexts."""
+    vox = sinusoid_field((20, 20, 20), seed=2)
+    i2o = np.array([0, 1, 0, -1, 0, 0, 0, 0, 1, 0, 0, 0], np.float32)
+    for kw in (dict(index_to_object=i2o), dict(cell_centered=True)):
+        vol = vkl.structured_regular(device, vox, **kw)
+        with pytest.raises(vkl.VKLError):
+            vkl.IntervalIteratorContext(vkl.Sampler(vol), macrocells=True)
+    vol = vkl.structured_regular(device, vox)
+    ctx = vkl.IntervalIteratorContext(vkl.Sampler(vol), macrocells=True)
+    with pytest.raises(vkl.VKLError):
+        ctx.iterate_one((0.5, 0.5, -1.0), (0.0, 0.0, 1.0), (0.0, np.inf))

@@ -317,3 +317,39 @@ def test_leaf_ranges_follow_reference_fold_order(oracle, background):
                 want.append(_reference_fold_leaf_range(vox, 8 * lx, 8 * ly, 8 * lz, background))
     want = np.array(want, np.float32)
     np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_macrocell_interval_continuity_and_ranges(oracle):
+    """The 16^3-voxel macrocell walk (the reference's legacy structuredRegular
+    iterator, GridAccelerator.ispc:146-240): the interval continuity assertion
+    of interval_iterator.cpp:108 (consecutive intervals share endpoints), the
+    first and last intervals at the box's entry and exit, nominalDeltaT =
+    min_i spacing_i / |dir_i| (GridAcceleratorIterator.ispc:76-78), and every
+    macrocell range equal to the min / max over its 17^3 clamped vertices."""
+    n = 70
+    vox = np.random.default_rng(0).random((n, n, n)).astype(np.float32)
+    v = oracle.OracleVolume.dense_volume(vox, grid_origin=(1.0, -2.0, 0.5), grid_spacing=(0.5, 0.5, 0.5))
+    rng = np.random.default_rng(2)
+    o = np.tile(np.array([[-10.0, 15.3, 17.7]], np.float32), (200, 1)) + rng.uniform(-2, 2, (200, 3)).astype(np.float32)
+    d = np.tile(np.array([[1.0, 0.0, 0.0]], np.float32), (200, 1)) + rng.uniform(-0.3, 0.3, (200, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = np.tile(np.array([[0, 1e30]], np.float32), (200, 1))
+    iv, cnt = v.macrocell_intervals(o, d, t, max_intervals=64)
+    lo = np.array([1.0, -2.0, 0.5])
+    hi = lo + (n - 1) * 0.5
+    for r in range(200):
+        k = int(cnt[r])
+        assert k > 0
+        ints = iv[r, :k]
+        assert np.all(ints[1:, 0] == ints[:-1, 1])
+        inv = 1.0 / d[r].astype(np.float64)
+        ta, tb = (lo - o[r]) * inv, (hi - o[r]) * inv
+        t0, t1 = np.max(np.minimum(ta, tb)), np.min(np.maximum(ta, tb))
+        assert ints[0, 0] == pytest.approx(t0, abs=1e-3)
+        assert ints[-1, 1] == pytest.approx(t1, abs=1e-3)
+        assert ints[0, 4] == pytest.approx(0.5 / np.max(np.abs(d[r])), rel=1e-6)
+    mr = v.macrocell_ranges()
+    assert mr.shape == (5, 5, 5, 2)
+    for cz, cy, cx in [(0, 0, 0), (4, 4, 4), (2, 3, 1), (4, 0, 2)]:
+        blk = vox[cz * 16:min(n, cz * 16 + 17), cy * 16:min(n, cy * 16 + 17), cx * 16:min(n, cx * 16 + 17)]
+        assert mr[cz, cy, cx, 0] == blk.min() and mr[cz, cy, cx, 1] == blk.max()
