@@ -411,7 +411,9 @@ OPENVKL_CUDA_INTERFACE void vklCudaReleaseSurrogate(VKLCudaSurrogate surrogate);
 // overlaps on one device share the scratch and race: issue them on one
 // stream.  The calling thread's current CUDA device must be the VKL
 // device's.  For volumes with NaN voxels the result may differ from the
-// committed volume's, whose NaN handling depends on reduction order.
+// committed volume's, whose NaN handling depends on reduction order; so may
+// the sign of a zero bound where +0.0 and -0.0 voxels meet (the two folds
+// visit them in different orders), which compares equal by value.
 // Returns VKL_NO_ERROR once launched, else the error code (also reported
 // through the device's error callback).
 OPENVKL_CUDA_INTERFACE VKLError vklCudaDenseValueRangeNoAlloc(VKLDevice device, const void *voxels,

@@ -27,7 +27,9 @@
 // the scratch address with cudaGetSymbolAddress, zeroes the counter, and
 // forces the kernels to load; all of this may make the driver load this
 // module's code and static memory, so the first call belongs before any
-// stream capture or allocation-free region.  Later calls only launch.
+// stream capture or allocation-free region.  Later calls look the address up
+// again (no allocation) and launch; a call whose launch fails makes the next
+// call repeat the set-up, which re-arms the counter.
 //
 // Concurrency.  All calls on one device share the one scratch array: two calls
 // whose launches overlap on the device (different streams, or threads)
@@ -154,7 +156,12 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
-// Per-device set-up: scratch address resolved once, with the device current.
+// Per-device set-up.  The scratch address is looked up on every call (a table
+// lookup once the module is loaded, no allocation) and compared with the one
+// the set-up was done for: a new context (after cudaDeviceReset, say) gets a
+// new address and so a new set-up.  A call whose launch reports an error
+// clears the cached address too, so the next call re-arms the counter: an
+// aborted launch may have left it counting.
 // ---------------------------------------------------------------------------
 std::mutex g_setupMutex;
 RangeScratch *g_scratch[kMaxDevices] = {};
@@ -166,6 +173,7 @@ void loadKernel()
   cudaCheck(cudaFuncGetAttributes(&attr, kDenseRangeNoAlloc<T>), "vklCudaDenseValueRangeNoAlloc set-up");
 }
 
+// The calling thread's current device must be `dev`.
 RangeScratch *scratchFor(int dev)
 {
   if (dev < 0 || dev >= kMaxDevices)
@@ -173,37 +181,31 @@ RangeScratch *scratchFor(int dev)
              " out of range",
          VKL_INVALID_ARGUMENT);
   std::lock_guard<std::mutex> lock(g_setupMutex);
-  if (g_scratch[dev])
-    return g_scratch[dev];
-  int cur = 0;
-  cudaCheck(cudaGetDevice(&cur), "vklCudaDenseValueRangeNoAlloc set-up: cudaGetDevice");
-  if (cur != dev)
-    cudaCheck(cudaSetDevice(dev), "vklCudaDenseValueRangeNoAlloc set-up: cudaSetDevice");
   RangeScratch *p = nullptr;
-  cudaError_t e   = cudaGetSymbolAddress((void **)&p, g_rangeScratch);
-  if (e == cudaSuccess)
-    e = cudaMemset(&p->blocksDone, 0, sizeof(unsigned int));
-  if (e == cudaSuccess)
-    e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) {
-    try {
-      loadKernel<uint8_t>();
-      loadKernel<int16_t>();
-      loadKernel<uint16_t>();
-      loadKernel<__half>();
-      loadKernel<float>();
-      loadKernel<double>();
-    } catch (...) {
-      if (cur != dev)
-        cudaSetDevice(cur);
-      throw;
-    }
-  }
-  if (cur != dev)
-    cudaSetDevice(cur);
-  cudaCheck(e, "vklCudaDenseValueRangeNoAlloc set-up: scratch symbol");
+  cudaCheck(cudaGetSymbolAddress((void **)&p, g_rangeScratch),
+            "vklCudaDenseValueRangeNoAlloc set-up: scratch symbol");
+  if (g_scratch[dev] == p)
+    return p;
+  g_scratch[dev] = nullptr;
+  cudaCheck(cudaMemset(&p->blocksDone, 0, sizeof(unsigned int)),
+            "vklCudaDenseValueRangeNoAlloc set-up: counter");
+  cudaCheck(cudaDeviceSynchronize(), "vklCudaDenseValueRangeNoAlloc set-up");
+  loadKernel<uint8_t>();
+  loadKernel<int16_t>();
+  loadKernel<uint16_t>();
+  loadKernel<__half>();
+  loadKernel<float>();
+  loadKernel<double>();
   g_scratch[dev] = p;
   return p;
+}
+
+// After a failed launch: the next call runs the set-up again.
+void forgetScratch(int dev)
+{
+  std::lock_guard<std::mutex> lock(g_setupMutex);
+  if (dev >= 0 && dev < kMaxDevices)
+    g_scratch[dev] = nullptr;
 }
 
 template <typename T>
@@ -249,7 +251,6 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaDenseValueRangeNoAlloc(
     default:
       fail("vklCudaDenseValueRangeNoAlloc: unsupported voxel type", VKL_INVALID_ARGUMENT);
     }
-    RangeScratch *s = scratchFor(d->cudaDevice);
     int cur = 0;
     cudaCheck(cudaGetDevice(&cur), "vklCudaDenseValueRangeNoAlloc: cudaGetDevice");
     if (cur != d->cudaDevice)
@@ -257,6 +258,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaDenseValueRangeNoAlloc(
                std::to_string(cur) + ") is not the VKL device's (" +
                std::to_string(d->cudaDevice) + ")",
            VKL_INVALID_OPERATION);
+    RangeScratch *s = scratchFor(d->cudaDevice);
     const int3 dims       = {dimX, dimY, dimZ};
     const unsigned blocks = (unsigned)((numLeaves + kThreads - 1) / kThreads);
     cudaStream_t st       = d->stream;
@@ -279,7 +281,11 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaDenseValueRangeNoAlloc(
     default:
       launch<float>(voxels, dims, nl, blocks, background, s, valueRange, st);
     }
-    cudaCheck(cudaGetLastError(), "vklCudaDenseValueRangeNoAlloc launch");
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      forgetScratch(d->cudaDevice);
+      cudaCheck(e, "vklCudaDenseValueRangeNoAlloc launch");
+    }
     return VKL_NO_ERROR;
   } catch (const VklError &e) {
     d->setError(e.code, e.what());

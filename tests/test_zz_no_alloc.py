@@ -105,3 +105,26 @@ def test_rejects_volumes_beyond_scratch(vkl, device):
                                              ctypes.c_void_p(out.data_ptr()))
     device.pending = None
     assert code == 2
+
+
+@pytest.mark.parametrize("dtype", [np.float16, np.float32, np.float64])
+def test_signed_zero_bounds_compare_by_value(vkl, device, dtype):
+    # A volume whose minimum is zero with both +0.0 and -0.0 voxels present:
+    # the two paths fold them in different orders, so the zero bound may come
+    # back with either sign bit; the ranges must be equal by value.
+    import torch
+    dims = (24, 20, 18)
+    vox = np.abs(_voxels(dims, np.float32, seed=3)).astype(dtype) + dtype(0.5)
+    vox[2:9, 3:7, 1:12] = dtype(0.0)
+    vox[4:6, 4:6, 2:10] = -dtype(0.0)
+    vox[15, 11, 20] = -dtype(0.0)
+    vol = vkl.structured_regular(device, vox)
+    expected = vol.value_range()
+    assert expected[0] == 0.0
+    d = _as_cuda(vox)
+    out = torch.empty(2, dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        vkl.dense_value_range_no_alloc(device, d, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert got[0] == expected[0] and got[1] == expected[1]  # by value: -0.0 == +0.0
