@@ -7,8 +7,8 @@ writes, for each of the 64 coefficients, the ordered list of
 (weight, constraint index) terms to tricubic_coeff_map.json.  The fixture
 pins the oracle's and the CUDA device's generated map to the reference.
 
-Run (where the reference tree exists):
-    python tests/golden/make_tricubic_golden.py /root/reference
+Run where the reference tree exists, naming its root:
+    python tests/golden/make_tricubic_golden.py <reference checkout>
 """
 import json
 import os
@@ -35,4 +35,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_tricubic_golden.py <reference checkout>")
+    main(sys.argv[1])
