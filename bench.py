@@ -280,7 +280,16 @@ def config_of(args):
                         + ("1920x1080 orbit-camera rays x 256 jittered samples" if args.workload != "incoherent"
                            else "2^26 uniform random points"),
             "points_per_step": n, "volume_bytes": DIMS[0] * DIMS[1] * DIMS[2] * 4,
-            "l2": "inputs larger than L2 (4 GiB volume, >=805 MB points), no flush"}
+            "l2": "inputs larger than L2 (4 GiB volume, >=805 MB points), no flush",
+            "parallelism": _parallelism(args)}
+
+
+def _parallelism(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return "1 GPU"
+    return (f"{ws} replicas, query partitioning (the points split across ranks)" if args.strong
+            else f"{ws} replicas, every rank samples the full point set")
 
 
 def run_cuda(args):
@@ -301,6 +310,12 @@ def run_cuda(args):
     f = FILTER[args.workload]
     smp = vkl.Sampler(vol, filter=f, gradient_filter=f)
     pts = points_torch(args.workload)
+    n_total = pts.shape[0]
+    if args.strong and ws > 1:
+        # strong scaling: the ranks split one point set (query partitioning)
+        from openvkl_b200.shard import query_slice
+        a, b = query_slice(n_total, rank, ws)
+        pts = pts[a:b].contiguous()
     n = pts.shape[0]
     grad = args.workload == "gradient"
     out = torch.empty((n, 3) if grad else (n,), dtype=torch.float32, device="cuda")
@@ -326,7 +341,8 @@ def run_cuda(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
         torch.distributed.barrier()
-    value = n * ws / (ms * 1e-3) / 1e9
+    job_points = n_total if (args.strong and ws > 1) else n * ws
+    value = job_points / (ms * 1e-3) / 1e9
 
     # algorithmic bytes of one launch: point in + result out + compulsory voxels
     io = n * (12 + (12 if grad else 4))
@@ -354,9 +370,19 @@ def run_cuda(args):
             tt = torch.tensor([e2e_s], device="cuda")
             torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
             e2e_s = float(tt.item())
-        e2e = {"value": n * ws / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 12,
+        e2e = {"value": job_points / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 12,
                "d2h_bytes_per_step": int(ho.numel()) * 4}
         del hp, ho
+
+    patterns = None
+    if rank == 0 and ws == 1 and args.workload == "coherent" and not args.no_patterns:
+        # the configs' other patterns, measured after the headline in the
+        # same process: the headline's buffers are released first
+        del vol, smp, tvox, pts, out, call
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        patterns = run_patterns(args)
 
     line = None
     if rank == 0:
@@ -370,7 +396,8 @@ def run_cuda(args):
                 traffic = tr["bytes_per_point"] * n
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if (args.strong and ws > 1) else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sinusoid volume, generated rays)",
             "config": config_of(args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -379,10 +406,56 @@ def run_cuda(args):
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps,
             "clocks": clocks,
         }
+        if patterns is not None:
+            line["patterns"] = patterns
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def run_patterns(args):
+    """Compact entries for the precision, batching and learned patterns,
+    each measured with CUDA events over a few steps of its own workload
+    (3 timed, 2 warm-up):
+      compressed  2^26 points in active leaves of the 4096^3 shell VDB:
+                  FP32 leaves vs FP16 / BF16 / FP8-E4M3 codes (per-leaf scale
+                  and offset), speed-up over FP32 and error against the FP64
+                  trilinear of the float leaves
+      batched     the 512-volume batch vs per-volume launches (eager and in
+                  a CUDA graph), sample + gradient of every point
+      learned     the hash-grid + MLP surrogate of the shell VDB, trained on
+                  2^28 points, against the plain sampler on 2^26 points"""
+    import argparse
+    import gc
+    import torch
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.collect = 3, 2, True
+    out = {}
+    v = run_vdb(sub)
+    out["compressed"] = {"workload": v["config"]["workload"], "unit": UNIT,
+                         "formats": {k: {x: f[x] for x in ("value", "speedup_vs_f32", "leaf_bytes",
+                                                          "fp64_max_abs_err_rel_range", "fp64_max_rel_err",
+                                                          "max_abs_err_rel_range") if x in f}
+                                     for k, f in v["formats"].items()}}
+    gc.collect()
+    torch.cuda.empty_cache()
+    b = run_batched(sub)
+    out["batched"] = {"workload": b["config"]["workload"], "unit": b["unit"], "batch": b["value"],
+                      "plain_eager": b["plain_eager"]["value"], "plain_graph": b["plain_graph"]["value"],
+                      "speedup_vs_plain_eager": b["speedup_vs_plain_eager"],
+                      "speedup_vs_plain_graph": b["speedup_vs_plain_graph"],
+                      "bit_exact_vs_plain": b["bit_exact_vs_plain"]}
+    gc.collect()
+    torch.cuda.empty_cache()
+    s = run_surrogate(sub)
+    out["learned"] = {"workload": s["config"]["workload"], "unit": UNIT, "surrogate_with_fallback": s["value"],
+                      "surrogate_no_fallback": s["surrogate_no_fallback"]["value"], "plain": s["plain"]["value"],
+                      "train_points_per_s": s["train"]["points_per_s"],
+                      "error_vs_plain": s["error_vs_plain"]}
+    gc.collect()
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_vdb_coherent(args):
@@ -412,13 +485,16 @@ def run_vdb(args, coherent=False):
     formats = np.ones(L, np.uint32)
     g = torch.Generator(device="cuda")
     g.manual_seed(11)
+    fp64 = None
     if coherent:
         pts = fields.orbit_camera_samples_torch(WIDTH, HEIGHT, 64, (0, 0, 0), (VDB_DOMAIN - 1,) * 3, seed=3)
     else:
         o_t = torch.from_numpy(origins).cuda()
         pick = torch.randint(0, L, (VDB_POINTS,), generator=g, device="cuda")
-        pts = (o_t[pick].to(torch.float32) + torch.rand((VDB_POINTS, 3), generator=g, device="cuda") * 8).contiguous()
-        del o_t, pick
+        loc = torch.rand((VDB_POINTS, 3), generator=g, device="cuda") * 8
+        pts = (o_t[pick].to(torch.float32) + loc).contiguous()
+        fp64 = _leaf_trilinear_fp64(values, pick, pts - o_t[pick].to(torch.float32))
+        del o_t, pick, loc
     npts = pts.shape[0]
     out = torch.empty(npts, dtype=torch.float32, device="cuda")
 
@@ -459,6 +535,12 @@ def run_vdb(args, coherent=False):
             r["max_abs_err_rel_range"] = float((out[ok] - ref[ok]).abs().max().item()) / vrange
             r["mean_abs_err_rel_range"] = float((out[ok] - ref[ok]).abs().mean().item()) / vrange
             r["speedup_vs_f32"] = results["f32"]["ms_per_step"] / ms
+        if fp64 is not None:
+            idx, want = fp64
+            e = (out[idx].to(torch.float64) - want).abs()
+            r["fp64_max_abs_err_rel_range"] = float(e.max().item()) / vrange
+            r["fp64_max_rel_err"] = float((e / want.abs().clamp_min(1e-3)).max().item())
+            r["fp64_points"] = int(idx.numel())
         results[fmt] = r
         del smp, vol
     line = {"metric": METRIC, "value": results["f32"]["value"], "unit": UNIT, "n_gpus": 1,
@@ -470,7 +552,32 @@ def run_vdb(args, coherent=False):
                                       else "2^26 points inside active leaves"),
                        "leaves": L, "points": npts},
             "formats": results}
+    if getattr(args, "collect", False):
+        return line
     print(json.dumps(line), flush=True)
+
+
+def _leaf_trilinear_fp64(values, leaf, local):
+    """FP64 trilinear of the float leaves (z fastest, 512 values per leaf) at
+    the points whose 2x2x2 stencil lies inside their own leaf (local
+    coordinates in [0, 7) on every axis): (indices of those points, FP64
+    samples)."""
+    import torch
+    inside = (local < 7).all(dim=1)
+    idx = torch.nonzero(inside).squeeze(1)
+    lc = local[idx].to(torch.float64)
+    i0 = torch.floor(lc).to(torch.int64)
+    f = lc - i0
+    base = leaf[idx].to(torch.int64) * 512
+    acc = torch.zeros(idx.numel(), dtype=torch.float64, device=local.device)
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                v = values[base + ((i0[:, 0] + dx) << 6) + ((i0[:, 1] + dy) << 3) + (i0[:, 2] + dz)]
+                w = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * \
+                    (f[:, 2] if dz else 1 - f[:, 2])
+                acc += w * v.to(torch.float64)
+    return idx, acc
 
 
 def run_batched(args):
@@ -550,9 +657,11 @@ def run_batched(args):
             "plain_graph": {"value": rate(ms_graph), "ms_per_step": ms_graph},
             "speedup_vs_plain_eager": ms_eager / ms_batch, "speedup_vs_plain_graph": ms_graph / ms_batch,
             "batch_config": batch.config(), "autotune_s": tune_s, "bit_exact_vs_plain": exact}
-    print(json.dumps(line), flush=True)
     batch.release()
     del graph
+    if getattr(args, "collect", False):
+        return line
+    print(json.dumps(line), flush=True)
 
 
 def _threaded_oracle(fn, n, threads, chunk=4096):
@@ -782,8 +891,10 @@ def run_surrogate(args):
             "calibration": {"threshold": 1e-2, "flagged_regions": flagged, "regions": sur.num_regions},
             "error_vs_plain": {"fallback": err(True), "no_fallback": err(False)},
             "gpu_launches": 3 * args.steps, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     sur.release()
+    if getattr(args, "collect", False):
+        return line
+    print(json.dumps(line), flush=True)
 
 
 def run_render(args):
@@ -998,6 +1109,11 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--workload", choices=list(FILTER), default="coherent")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--strong", action="store_true",
+                    help="with --gpus N > 1: the ranks split the one point set (query partitioning) "
+                         "instead of each sampling all of it")
+    ap.add_argument("--no-patterns", action="store_true",
+                    help="default workload: skip the compressed / batched / learned pattern entries")
     ap.add_argument("--no-extras", action="store_true",
                     help="timed loop only (no e2e / roofline bytes / CPU baseline): profiling runs")
     ap.add_argument("--small", action="store_true",
@@ -1011,6 +1127,7 @@ def main(argv=None):
         VDB_DOMAIN, VDB_POINTS, HIT_RAYS, TRAIN_STEPS = 2048, 1 << 24, 1 << 20, 64
     if args.no_extras:
         args.no_cpu_baseline = True
+        args.no_patterns = True
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "vdb":

@@ -6,6 +6,9 @@
 // (openvkl/api/API.cpp:37-89, devices/cpu/api/DeviceAPI.cpp:25-57).
 #include <algorithm>
 #include <cmath>
+#include <cctype>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <mutex>
@@ -297,6 +300,84 @@ struct IterHeader {
   ManagedObject *context;
 };
 
+// The reference device's default callbacks (Device.cpp:27-54): log
+// messages go to stdout as they are, errors to stderr as
+// "OPENVKL ERROR [<code>]: <message>".
+void logToStdout(void *, const char *msg) { std::fputs(msg, stdout); }
+void logToStderr(void *, const char *msg) { std::fputs(msg, stderr); }
+void logToNowhere(void *, const char *) {}
+void errorToStderr(void *, VKLError e, const char *msg)
+{
+  std::fprintf(stderr, "OPENVKL ERROR [%d]: %s\n", (int)e, msg);
+}
+void errorToStdout(void *, VKLError e, const char *msg)
+{
+  std::fprintf(stdout, "OPENVKL ERROR [%d]: %s\n", (int)e, msg);
+  std::fflush(stdout);
+}
+void errorToNowhere(void *, VKLError, const char *) {}
+
+std::string lowerCase(std::string s)
+{
+  for (char &c : s)
+    c = (char)std::tolower((unsigned char)c);
+  return s;
+}
+
+// Device::commit (Device.cpp:135-199): the logLevel / logOutput /
+// errorOutput parameters, each overridden by its OPENVKL_* environment
+// variable.  OPENVKL_THREADS / numThreads and OPENVKL_FLUSH_DENORMALS /
+// flushDenormals configure the reference's host tasking system; the cuda
+// device has none, so they are read and ignored.
+void configureFromEnvironment(Device *d)
+{
+  auto ip = d->intParams.find("logLevel");
+  d->logLevel = ip != d->intParams.end() ? ip->second : VKL_LOG_INFO;
+  if (const char *e = std::getenv("OPENVKL_LOG_LEVEL")) {
+    const std::string v = lowerCase(e);
+    if (v == "debug")
+      d->logLevel = VKL_LOG_DEBUG;
+    else if (v == "info")
+      d->logLevel = VKL_LOG_INFO;
+    else if (v == "warning")
+      d->logLevel = VKL_LOG_WARNING;
+    else if (v == "error")
+      d->logLevel = VKL_LOG_ERROR;
+    else if (v == "none")
+      d->logLevel = VKL_LOG_NONE;
+    else if (!v.empty())
+      d->log(VKL_LOG_ERROR, "unknown OPENVKL_LOG_LEVEL env value; must be debug, info, warning, error or none");
+  }
+  auto param = [&](const char *name) {
+    auto it = d->stringParams.find(name);
+    return it == d->stringParams.end() ? std::string() : it->second;
+  };
+  const char *lo = std::getenv("OPENVKL_LOG_OUTPUT");
+  const std::string logDst = lo ? std::string(lo) : param("logOutput");
+  if (logDst == "cout") {
+    d->logCb   = logToStdout;
+    d->logUser = nullptr;
+  } else if (logDst == "cerr") {
+    d->logCb   = logToStderr;
+    d->logUser = nullptr;
+  } else if (logDst == "none") {
+    d->logCb   = logToNowhere;
+    d->logUser = nullptr;
+  }
+  const char *eo = std::getenv("OPENVKL_ERROR_OUTPUT");
+  const std::string errDst = eo ? std::string(eo) : param("errorOutput");
+  if (errDst == "cout") {
+    d->errorCb   = errorToStdout;
+    d->errorUser = nullptr;
+  } else if (errDst == "cerr") {
+    d->errorCb   = errorToStderr;
+    d->errorUser = nullptr;
+  } else if (errDst == "none") {
+    d->errorCb   = errorToNowhere;
+    d->errorUser = nullptr;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -318,6 +399,8 @@ VKLDevice vklNewDevice(const char *name)
     }
     Device *d = new Device();
     cudaGetDevice(&d->cudaDevice);
+    d->logCb   = logToStdout;
+    d->errorCb = errorToStderr;
     std::lock_guard<std::mutex> lock(g_devicesMutex);
     g_lastDevice = d;
     return (VKLDevice)d;
@@ -387,6 +470,7 @@ void vklCommitDevice(VKLDevice dev)
       d->cudaDevice = it->second;
       cudaCheck(cudaSetDevice(d->cudaDevice), "cudaSetDevice");
     }
+    configureFromEnvironment(d);
     d->committed = true;
   });
 }
