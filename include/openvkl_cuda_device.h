@@ -20,8 +20,10 @@
 // skip the excluded paths, and drop them from the inlined code when the
 // argument is a compile-time constant.  VKL_FEATURE_FLAGS_DEFAULT (all bits)
 // and 0 keep every path.  Results are identical either way.  The iterators
-// accept the flags and do not need them.  `time` is ignored (no temporal
-// formats).
+// accept the flags and do not need them.  `time` is the sample time of
+// temporally varying structuredRegular volumes (feature flags
+// VKL_FEATURE_FLAG_HAS_TEMPORAL_FORMAT_STRUCTURED / _UNSTRUCTURED, bits 13 and
+// 14); other volumes ignore it.
 //
 // Results are bit-identical to the host API's when the including
 // translation unit is compiled like the library: nvcc -gencode
@@ -45,6 +47,7 @@ struct IntervalIteratorState {
 struct HitIteratorState {
   HitIt h;
   const DevHitContextState *ctx;
+  float time;
 };
 static_assert(sizeof(IntervalIteratorState) <= VKL_CUDA_INTERVAL_ITERATOR_SIZE, "interval iterator size");
 static_assert(sizeof(HitIteratorState) <= VKL_CUDA_HIT_ITERATOR_SIZE, "hit iterator size");
@@ -54,14 +57,18 @@ __device__ __forceinline__ f3 toF3(const vkl_vec3f *v) { return {v->x, v->y, v->
 constexpr VKLFeatureFlags kStructuredRegular = 1ull << 0, kVdb = 1ull << 5;
 constexpr VKLFeatureFlags kSampleNearest = 1ull << 6, kSampleLinear = 1ull << 7, kSampleCubic = 1ull << 8;
 constexpr VKLFeatureFlags kGradientNearest = 1ull << 9, kGradientLinear = 1ull << 10, kGradientCubic = 1ull << 11;
+constexpr VKLFeatureFlags kTemporalVarying = (1ull << 13) | (1ull << 14);
 
 // Runs f(field) with the sampler's field type, over the volume kinds the
 // flags allow (the type dispatch of sampleIndexAny).
 template <class F>
-__device__ __forceinline__ auto withField(const DevGrid &g, uint32_t attr, uint32_t depth, VKLFeatureFlags ff, F &&f)
+__device__ __forceinline__ auto withField(const DevGrid &g, uint32_t attr, uint32_t depth, VKLFeatureFlags ff, F &&f,
+                                          float time = 0.f)
 {
   const bool denseOk = ff & kStructuredRegular, vdbOk = ff & kVdb;
   const uint32_t t   = g.type[attr];
+  if ((ff & kTemporalVarying) && g.temporal)
+    return withTemporalField(g, attr, time, f);
   if (denseOk && (g.dense || !vdbOk)) {
     switch (t) {
     case kUChar:
@@ -103,7 +110,7 @@ __device__ __forceinline__ bool atlasLinear(const DevGrid &g, int filter, uint32
 }
 
 __device__ __forceinline__ float sample(const DevGrid &g, int filter, uint32_t depth, uint32_t attr, f3 oc,
-                                        VKLFeatureFlags ff)
+                                        VKLFeatureFlags ff, float time = 0.f)
 {
   if (ff == 0)
     ff = ~0ull;
@@ -111,16 +118,20 @@ __device__ __forceinline__ float sample(const DevGrid &g, int filter, uint32_t d
   if (atlasLinear(g, filter, attr, ff, kSampleLinear))
     return sampleLinear(AtlasField(g, attr), p);
   const bool cc = g.constantCellData != 0;
-  return withField(g, attr, depth, ff, [&](const auto &F) -> float {
-    if ((ff & kSampleNearest) && filter == kFilterNearest)
-      return sampleNearest(F, cc, p);
-    if ((ff & kSampleCubic) && filter == kFilterCubic)
-      return sampleCubic(F, p);
-    return sampleLinear(F, p);
-  });
+  return withField(
+      g, attr, depth, ff,
+      [&](const auto &F) -> float {
+        if ((ff & kSampleNearest) && filter == kFilterNearest)
+          return sampleNearest(F, cc, p);
+        if ((ff & kSampleCubic) && filter == kFilterCubic)
+          return sampleCubic(F, p);
+        return sampleLinear(F, p);
+      },
+      time);
 }
 
-__device__ __forceinline__ f3 gradient(const DevSamplerState *st, uint32_t attr, f3 oc, VKLFeatureFlags ff)
+__device__ __forceinline__ f3 gradient(const DevSamplerState *st, uint32_t attr, f3 oc, VKLFeatureFlags ff,
+                                       float time = 0.f)
 {
   if (ff == 0)
     ff = ~0ull;
@@ -131,10 +142,14 @@ __device__ __forceinline__ f3 gradient(const DevSamplerState *st, uint32_t attr,
   const f3 p = xfmPoint(g.objectToIndex, oc);
   if (atlasLinear(g, filter, attr, ff, kGradientLinear))
     return xfmNormal(g.objectToIndex, gradientLinear(AtlasField(g, attr), p));
-  return withField(g, attr, st->s.maxSamplingDepth, ff, [&](const auto &F) -> f3 {
-    const f3 gi = ((ff & kGradientCubic) && filter == kFilterCubic) ? gradientCubic(F, p) : gradientLinear(F, p);
-    return xfmNormal(g.objectToIndex, gi);
-  });
+  return withField(
+      g, attr, st->s.maxSamplingDepth, ff,
+      [&](const auto &F) -> f3 {
+        const f3 gi =
+            ((ff & kGradientCubic) && filter == kFilterCubic) ? gradientCubic(F, p) : gradientLinear(F, p);
+        return xfmNormal(g.objectToIndex, gi);
+      },
+      time);
 }
 
 }  // namespace device_api
@@ -145,10 +160,9 @@ __device__ inline float vklComputeSample(const VKLSampler *sampler, const vkl_ve
                                          unsigned int attributeIndex, float time,
                                          const VKLFeatureFlags featureFlags)
 {
-  (void)time;
   const auto *st = (const vklcuda::DevSamplerState *)sampler->device;
   return vklcuda::device_api::sample(st->g, st->s.filter, st->s.maxSamplingDepth, attributeIndex,
-                                     vklcuda::device_api::toF3(objectCoordinates), featureFlags);
+                                     vklcuda::device_api::toF3(objectCoordinates), featureFlags, time);
 }
 
 // Samples of M attributes (vklComputeSampleM).
@@ -165,10 +179,9 @@ __device__ inline vkl_vec3f vklComputeGradient(const VKLSampler *sampler, const 
                                                unsigned int attributeIndex, float time,
                                                const VKLFeatureFlags featureFlags)
 {
-  (void)time;
   const vklcuda::f3 r = vklcuda::device_api::gradient((const vklcuda::DevSamplerState *)sampler->device,
                                                       attributeIndex, vklcuda::device_api::toF3(objectCoordinates),
-                                                      featureFlags);
+                                                      featureFlags, time);
   return vkl_vec3f{r.x, r.y, r.z};
 }
 
@@ -210,10 +223,10 @@ __device__ inline VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext 
                                                     const vkl_vec3f *direction, const vkl_range1f *tRange,
                                                     float time, void *buffer, const VKLFeatureFlags featureFlags)
 {
-  (void)time;
   (void)featureFlags;
   auto *s = (vklcuda::device_api::HitIteratorState *)buffer;
   s->ctx  = (const vklcuda::DevHitContextState *)context->device;
+  s->time = time;
   vklcuda::hitInit(s->ctx->sampler->g, s->ctx->depth, vklcuda::device_api::toF3(origin),
                    vklcuda::device_api::toF3(direction), tRange->lower, tRange->upper, s->h);
   return (VKLHitIterator)buffer;
@@ -229,7 +242,7 @@ __device__ inline int vklIterateHit(VKLHitIterator iterator, VKLHit *hit, const 
   // the march samples through the generic sampler, out of line (one copy
   // for every sampling site of the march and bisection)
   if (!vklcuda::hitNext(g, c->sampler->s.filter, c->attr, vklcuda::kNumLevels - 1, c->vr, c->numValues,
-                        c->values, s->h, h))
+                        c->values, s->h, h, s->time))
     return 0;
   hit->t       = h.t;
   hit->sample  = h.sample;

@@ -212,8 +212,44 @@ bool binned(Device *d, Sampler *s, int filter, uint64_t n, const float *pts, uin
   return launchSampleBinned(g, filter, n, pts, attr, out, grad, d->binScratch, d->stream);
 }
 
+// Temporally varying volumes: points, times and results staged through the
+// device buffers in one piece (no copy pipeline), one kernel launch.
+void sampleTemporal(Device *d, Sampler *s, uint64_t N, const void *pts, const float *times, void *out,
+                    uint32_t M, const uint32_t *attrs, bool grad)
+{
+  const DevGrid &g        = s->launchGrid();
+  const int filter        = grad ? s->s.gradientFilter : s->s.filter;
+  const size_t outStride  = grad ? 12 : 4 * (size_t)M;
+  const bool ptsDev = isDevicePtr(pts), outDev = isDevicePtr(out), tDev = !times || isDevicePtr(times);
+  if (ptsDev && outDev && tDev) {
+    launchSampleTemporal(g, filter, N, (const float *)pts, times, M, attrs, (float *)out, grad, d->stream);
+    return;
+  }
+  std::lock_guard<std::mutex> lock(d->stagingMutex);
+  d->stageIn.reserve(N * 16);
+  d->stageOut.reserve(N * outStride);
+  const float *dp = (const float *)pts, *dt = times;
+  if (!ptsDev) {
+    cudaCheck(cudaMemcpyAsync(d->stageIn.ptr, pts, N * 12, cudaMemcpyHostToDevice, d->stream), "stage in");
+    dp = d->stageIn.as<float>();
+  }
+  if (!tDev) {
+    float *slot = (float *)(d->stageIn.as<uint8_t>() + N * 12);
+    cudaCheck(cudaMemcpyAsync(slot, times, N * 4, cudaMemcpyHostToDevice, d->stream), "stage in");
+    dt = slot;
+  }
+  float *dout = outDev ? (float *)out : d->stageOut.as<float>();
+  launchSampleTemporal(g, filter, N, dp, dt, M, attrs, dout, grad, d->stream);
+  if (!outDev)
+    cudaCheck(cudaMemcpyAsync(out, dout, N * outStride, cudaMemcpyDeviceToHost, d->stream), "stage out");
+  cudaCheck(cudaStreamSynchronize(d->stream), "synchronize");
+}
+
+// `times`: one time per point (host or device memory), or NULL for time 0;
+// only temporally varying volumes read them (the reference's temporally
+// constant volumes ignore the time as well).
 void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float *out,
-             uint32_t M, const uint32_t *attrs)
+             uint32_t M, const uint32_t *attrs, const float *times = nullptr)
 {
   Sampler *s = committedSampler(sampler);
   if (M == 0 || M > kMaxAttributes)
@@ -226,6 +262,10 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
   if (!pts || !out)
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
+  if (s->volume->grid.temporal) {
+    sampleTemporal(d, s, N, pts, times, out, M, attrs, false);
+    return;
+  }
   staged(d, N, 12, pts, 4 * M, out, [&](uint64_t n, const void *din, void *dout) {
     if (M == 1 && binned(d, s, s->s.filter, n, (const float *)din, attrs[0], (float *)dout, false))
       return;
@@ -235,7 +275,7 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
 }
 
 void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_vec3f *out,
-               uint32_t attr)
+               uint32_t attr, const float *times = nullptr)
 {
   Sampler *s = committedSampler(sampler);
   if (attr >= s->volume->grid.numAttributes)
@@ -245,6 +285,10 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
   if (!pts || !out)
     fail("NULL coordinates or output", VKL_INVALID_ARGUMENT);
   Device *d = s->device;
+  if (s->volume->grid.temporal) {
+    sampleTemporal(d, s, N, pts, times, out, 1, &attr, true);
+    return;
+  }
   staged(d, N, 12, pts, 12, out, [&](uint64_t n, const void *din, void *dout) {
     if (binned(d, s, s->s.gradientFilter, n, (const float *)din, attr, (float *)dout, true))
       return;
@@ -255,35 +299,40 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
 
 template <int W, class V>
 void sampleW(const int *valid, const VKLSampler *sampler, const V *oc, float *samples,
-             uint32_t M, const uint32_t *attrs)
+             uint32_t M, const uint32_t *attrs, const float *times)
 {
   vkl_vec3f pts[W];
+  float tm[W];
   int idx[W];
   int n = 0;
   for (int i = 0; i < W; ++i)
     if (!valid || valid[i]) {
       pts[n] = {oc->x[i], oc->y[i], oc->z[i]};
+      tm[n]  = times ? times[i] : 0.f;
       idx[n++] = i;
     }
   std::vector<float> out((size_t)W * M);
-  sampleN(sampler, (uint64_t)n, pts, out.data(), M, attrs);
+  sampleN(sampler, (uint64_t)n, pts, out.data(), M, attrs, tm);
   for (int k = 0; k < n; ++k)
     for (uint32_t m = 0; m < M; ++m)
       samples[m * W + idx[k]] = out[k * M + m];
 }
 
 template <int W, class V>
-void gradientW(const int *valid, const VKLSampler *sampler, const V *oc, V *grads, uint32_t attr)
+void gradientW(const int *valid, const VKLSampler *sampler, const V *oc, V *grads, uint32_t attr,
+               const float *times)
 {
   vkl_vec3f pts[W], out[W];
+  float tm[W];
   int idx[W];
   int n = 0;
   for (int i = 0; i < W; ++i)
     if (!valid || valid[i]) {
       pts[n] = {oc->x[i], oc->y[i], oc->z[i]};
+      tm[n]  = times ? times[i] : 0.f;
       idx[n++] = i;
     }
-  gradientN(sampler, (uint64_t)n, pts, out, attr);
+  gradientN(sampler, (uint64_t)n, pts, out, attr, tm);
   for (int k = 0; k < n; ++k) {
     grads->x[idx[k]] = out[k].x;
     grads->y[idx[k]] = out[k].y;
@@ -721,7 +770,10 @@ VKLFeatureFlags vklGetFeatureFlags(VKLSampler sampler)
                                           : (1u << (base + 2));
         };
         ff |= filterBit(s->s.filter, 6) | filterBit(s->s.gradientFilter, 9);
-        ff |= 1u << 12;  // temporally constant
+        // temporal format (VKLFeatureFlagsInternal.h:32-34): constant,
+        // structured or unstructured
+        const uint32_t tf = s->volume->grid.temporal;
+        ff |= tf == 1 ? (1u << 13) : tf == 2 ? (1u << 14) : (1u << 12);
         ff |= (s->volume->isDense || !s->volume->has("nodesPackedDense")) ? (1u << 20) : (1u << 19);
         return ff;
       },
@@ -732,109 +784,109 @@ VKLFeatureFlags vklGetFeatureFlags(VKLSampler sampler)
 // Sampling.
 // ---------------------------------------------------------------------------
 float vklComputeSample(const VKLSampler *sampler, const vkl_vec3f *oc, unsigned int attr,
-                       float /*time*/)
+                       float time)
 {
   return guarded(
       sampler ? deviceOf(*sampler) : g_lastDevice,
       [&]() -> float {
         float out = kNaN;
-        sampleN(sampler, 1, oc, &out, 1, &attr);
+        sampleN(sampler, 1, oc, &out, 1, &attr, &time);
         return out;
       },
       kNaN);
 }
 
 void vklComputeSample4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc,
-                       float *samples, unsigned int attr, const float *)
+                       float *samples, unsigned int attr, const float *times)
 {
   guardedVoid(s ? deviceOf(*s) : g_lastDevice,
-              [&]() { sampleW<4>(valid, s, oc, samples, 1, &attr); });
+              [&]() { sampleW<4>(valid, s, oc, samples, 1, &attr, times); });
 }
 void vklComputeSample8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc,
-                       float *samples, unsigned int attr, const float *)
+                       float *samples, unsigned int attr, const float *times)
 {
   guardedVoid(s ? deviceOf(*s) : g_lastDevice,
-              [&]() { sampleW<8>(valid, s, oc, samples, 1, &attr); });
+              [&]() { sampleW<8>(valid, s, oc, samples, 1, &attr, times); });
 }
 void vklComputeSample16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc,
-                        float *samples, unsigned int attr, const float *)
+                        float *samples, unsigned int attr, const float *times)
 {
   guardedVoid(s ? deviceOf(*s) : g_lastDevice,
-              [&]() { sampleW<16>(valid, s, oc, samples, 1, &attr); });
+              [&]() { sampleW<16>(valid, s, oc, samples, 1, &attr, times); });
 }
 
 void vklComputeSampleM4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc, float *samples,
-                        unsigned int M, const unsigned int *attrs, const float *)
+                        unsigned int M, const unsigned int *attrs, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<4>(valid, s, oc, samples, M, attrs); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<4>(valid, s, oc, samples, M, attrs, times); });
 }
 void vklComputeSampleM8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc, float *samples,
-                        unsigned int M, const unsigned int *attrs, const float *)
+                        unsigned int M, const unsigned int *attrs, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<8>(valid, s, oc, samples, M, attrs); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<8>(valid, s, oc, samples, M, attrs, times); });
 }
 void vklComputeSampleM16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc, float *samples,
-                         unsigned int M, const unsigned int *attrs, const float *)
+                         unsigned int M, const unsigned int *attrs, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<16>(valid, s, oc, samples, M, attrs); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { sampleW<16>(valid, s, oc, samples, M, attrs, times); });
 }
 
 void vklComputeGradient4(const int *valid, const VKLSampler *s, const vkl_vvec3f4 *oc, vkl_vvec3f4 *grads,
-                         unsigned int attr, const float *)
+                         unsigned int attr, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<4>(valid, s, oc, grads, attr); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<4>(valid, s, oc, grads, attr, times); });
 }
 void vklComputeGradient8(const int *valid, const VKLSampler *s, const vkl_vvec3f8 *oc, vkl_vvec3f8 *grads,
-                         unsigned int attr, const float *)
+                         unsigned int attr, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<8>(valid, s, oc, grads, attr); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<8>(valid, s, oc, grads, attr, times); });
 }
 void vklComputeGradient16(const int *valid, const VKLSampler *s, const vkl_vvec3f16 *oc,
-                          vkl_vvec3f16 *grads, unsigned int attr, const float *)
+                          vkl_vvec3f16 *grads, unsigned int attr, const float *times)
 {
-  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<16>(valid, s, oc, grads, attr); });
+  guardedVoid(s ? deviceOf(*s) : g_lastDevice, [&]() { gradientW<16>(valid, s, oc, grads, attr, times); });
 }
 
 void vklComputeSampleN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
-                       float *samples, unsigned int attr, const float * /*times*/)
+                       float *samples, unsigned int attr, const float *times)
 {
   guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
-              [&]() { sampleN(sampler, N, oc, samples, 1, &attr); });
+              [&]() { sampleN(sampler, N, oc, samples, 1, &attr, times); });
 }
 
 void vklComputeSampleM(const VKLSampler *sampler, const vkl_vec3f *oc, float *samples,
-                       unsigned int M, const unsigned int *attrs, float /*time*/)
+                       unsigned int M, const unsigned int *attrs, float time)
 {
   guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
-              [&]() { sampleN(sampler, 1, oc, samples, M, attrs); });
+              [&]() { sampleN(sampler, 1, oc, samples, M, attrs, &time); });
 }
 
 void vklComputeSampleMN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
                         float *samples, unsigned int M, const unsigned int *attrs,
-                        const float * /*times*/)
+                        const float *times)
 {
   guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
-              [&]() { sampleN(sampler, N, oc, samples, M, attrs); });
+              [&]() { sampleN(sampler, N, oc, samples, M, attrs, times); });
 }
 
 vkl_vec3f vklComputeGradient(const VKLSampler *sampler, const vkl_vec3f *oc, unsigned int attr,
-                             float /*time*/)
+                             float time)
 {
   return guarded(
       sampler ? deviceOf(*sampler) : g_lastDevice,
       [&]() -> vkl_vec3f {
         vkl_vec3f g{kNaN, kNaN, kNaN};
-        gradientN(sampler, 1, oc, &g, attr);
+        gradientN(sampler, 1, oc, &g, attr, &time);
         return g;
       },
       vkl_vec3f{kNaN, kNaN, kNaN});
 }
 
 void vklComputeGradientN(const VKLSampler *sampler, unsigned int N, const vkl_vec3f *oc,
-                         vkl_vec3f *gradients, unsigned int attr, const float * /*times*/)
+                         vkl_vec3f *gradients, unsigned int attr, const float *times)
 {
   guardedVoid(sampler ? deviceOf(*sampler) : g_lastDevice,
-              [&]() { gradientN(sampler, N, oc, gradients, attr); });
+              [&]() { gradientN(sampler, N, oc, gradients, attr, times); });
 }
 
 // ---------------------------------------------------------------------------
@@ -957,7 +1009,7 @@ int vklIterateInterval(VKLIntervalIterator iterator, VKLInterval *interval)
 
 VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context, const vkl_vec3f *origin,
                                   const vkl_vec3f *direction, const vkl_range1f *tRange,
-                                  float /*time*/, void *buffer)
+                                  float time, void *buffer)
 {
   return guarded(
       context ? deviceOf(*context) : g_lastDevice,
@@ -969,8 +1021,10 @@ VKLHitIterator vklInitHitIterator(const VKLHitIteratorContext *context, const vk
         IterHeader *h      = (IterHeader *)buffer;
         h->magic           = kHitMagic;
         h->context         = c;
-        const float ray[8] = {origin->x, origin->y, origin->z, direction->x, direction->y,
-                              direction->z, tRange->lower, tRange->upper};
+        // the ray, its t range and the time its samples are taken at
+        // (temporally varying volumes)
+        const float ray[9] = {origin->x, origin->y, origin->z, direction->x, direction->y,
+                              direction->z, tRange->lower, tRange->upper, time};
         std::lock_guard<std::mutex> lock(d->stagingMutex);
         const size_t ss = hitIterStateSize();
         d->stageAux.reserve(ss + 64);

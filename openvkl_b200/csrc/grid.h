@@ -154,6 +154,16 @@ struct DevGrid {
   // side by side in the atlas, a few KB apart.
   uint64_t atlasTex[kMaxAttributes];
   uint32_t atlasPlanesPerRow;
+  // Temporally varying (motion-blur) dense data, kept as given (x fastest,
+  // each voxel's time samples consecutive, not bricked): 0 = constant,
+  // 1 = structured (numTimesteps values per voxel, regularly placed in
+  // [0, 1]), 2 = unstructured (voxel v's samples are data[idx[v] ..
+  // idx[v+1]) at times[idx[v] .. idx[v+1]), idx 32- or 64-bit).
+  uint32_t temporal;
+  uint32_t numTimesteps;
+  uint32_t tIndex64;
+  const void *tIndices;
+  const float *tTimes;
 };
 
 struct DevSampler {

@@ -336,9 +336,9 @@ __device__ inline bool intervalNext(const DevGrid &g, uint32_t attr, const DevVa
 // type / filter dispatch (static: one copy per translation unit that
 // includes this header).
 static __device__ __noinline__ float hitSample(const DevGrid &g, int filter, uint32_t attr, uint32_t depth,
-                                        f3 p)
+                                        f3 p, float time)
 {
-  return sampleObjectAny(g, filter, attr, depth, p);
+  return sampleObjectAny(g, filter, attr, depth, p, time);
 }
 
 // Sample hooks of the hit iterator's marching.  AnySampleHook dispatches on
@@ -351,7 +351,8 @@ struct AnySampleHook {
   int filter;
   uint32_t attr;
   uint32_t depth;
-  __device__ __forceinline__ float operator()(f3 oc) const { return hitSample(*g, filter, attr, depth, oc); }
+  float time = 0.f;  // the iterator's time (temporally varying volumes)
+  __device__ __forceinline__ float operator()(f3 oc) const { return hitSample(*g, filter, attr, depth, oc, time); }
 };
 
 template <class Field>
@@ -802,9 +803,10 @@ __device__ inline void hitsAllLanes(const DevGrid &g, const Hook &hook, uint32_t
 
 __device__ inline bool hitNext(const DevGrid &g, int filter, uint32_t attr, uint32_t sampleDepth,
                                const DevValueRanges &vr, uint32_t numValues, const float *values,
-                               HitIt &h, DevHit &hit)
+                               HitIt &h, DevHit &hit, float time = 0.f)
 {
-  return hitNextWith<1>(g, AnySampleHook{&g, filter, attr, sampleDepth}, attr, vr, numValues, values, h, hit);
+  return hitNextWith<1>(g, AnySampleHook{&g, filter, attr, sampleDepth, time}, attr, vr, numValues, values, h,
+                        hit);
 }
 
 }  // namespace vklcuda

@@ -283,7 +283,7 @@ int classOf(const Sampler *s, bool wantGrad, uint32_t attr)
       return kDenseF32;
     }
   }
-  if (g.compress != kCompressNone || s->s.maxSamplingDepth < kNumLevels - 1)
+  if (g.compress != kCompressNone || g.temporal || s->s.maxSamplingDepth < kNumLevels - 1)
     return -1;
   return g.type[attr] == kHalf ? kSparseF16 : kSparseF32;
 }

@@ -275,7 +275,7 @@ BinGrid binGridOf(const DevGrid &g)
 
 bool binnedSamplingApplies(const DevGrid &g, int filter, uint64_t n, uint32_t attr)
 {
-  if (!g.dense || g.type[attr] != kFloat || n < kBinMinPts)
+  if (!g.dense || g.temporal || g.type[attr] != kFloat || n < kBinMinPts)
     return false;
   // trilinear taps from a texture atlas need no binning: the texture path
   // takes incoherent points faster unsorted (16.6 vs 13-14 Gsamples/s on

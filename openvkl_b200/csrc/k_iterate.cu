@@ -99,6 +99,7 @@ struct IntervalIterStateImpl {
 };
 struct HitIterStateImpl {
   uint32_t attr;
+  float time;
   HitIt h;
 };
 
@@ -123,6 +124,7 @@ __global__ void kHitIterInit(const __grid_constant__ DevGrid g, uint32_t attr, u
                              const float *ray, HitIterStateImpl *s)
 {
   s->attr = attr;
+  s->time = ray[8];
   hitInit(g, depth, {ray[0], ray[1], ray[2]}, {ray[3], ray[4], ray[5]}, ray[6], ray[7], s->h);
 }
 
@@ -131,7 +133,7 @@ __global__ void kHitIterNext(const __grid_constant__ DevGrid g, int filter, DevV
                              DevHit *out, int *result)
 {
   DevHit hit;
-  const bool ok = hitNext(g, filter, s->attr, kNumLevels - 1, vr, numValues, values, s->h, hit);
+  const bool ok = hitNext(g, filter, s->attr, kNumLevels - 1, vr, numValues, values, s->h, hit, s->time);
   if (ok)
     *out = hit;
   *result = ok ? 1 : 0;
@@ -160,7 +162,7 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
 {
   if (!n)
     return;
-  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && g.compress == kCompressNone;
+  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && g.compress == kCompressNone && !g.temporal;
   auto k         = kHits<kHitAny, 1>;
   if (lin && g.dense)
     k = kHits<kHitDenseFloatLinear, kHitLookahead>;

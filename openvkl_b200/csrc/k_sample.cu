@@ -42,6 +42,10 @@ void launchSample(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
                   const float *points, uint32_t M, const uint32_t *attrs, float *out,
                   cudaStream_t stream)
 {
+  if (g.temporal) {  // temporally varying data, sampled at time 0
+    launchSampleTemporal(g, filter, n, points, nullptr, M, attrs, out, false, stream);
+    return;
+  }
   if (M == 1) {
     dispatch(g, filter, maxDepth, n, points, attrs[0], out, false, stream);
   } else if (n) {
@@ -57,6 +61,10 @@ void launchSample(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
 void launchGradient(const DevGrid &g, int filter, uint32_t maxDepth, uint64_t n,
                     const float *points, uint32_t attr, float *out, cudaStream_t stream)
 {
+  if (g.temporal) {
+    launchSampleTemporal(g, filter, n, points, nullptr, 1, &attr, out, true, stream);
+    return;
+  }
   dispatch(g, filter, maxDepth, n, points, attr, out, true, stream);
   cudaCheck(cudaGetLastError(), "gradient kernel launch");
 }

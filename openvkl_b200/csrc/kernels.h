@@ -66,6 +66,13 @@ void launchIntervals(const DevGrid &g, uint32_t attr, uint32_t depth, DevValueRa
                      uint64_t n, const float *origins, const float *directions,
                      const float *tRanges, uint32_t maxPerRay, DevInterval *out,
                      uint32_t *counts, cudaStream_t stream);
+// Temporally varying dense volumes (k_temporal.cu): samples / gradients at
+// per-point times (times NULL: time 0; M > 1: samples of M attributes) and
+// the commit's leaf value ranges over all time samples.
+void launchSampleTemporal(const DevGrid &g, int filter, uint64_t n, const float *points, const float *times,
+                          uint32_t M, const uint32_t *attrs, float *out, bool grad, cudaStream_t stream);
+void launchTemporalLeafRanges(const DevGrid &g, uint32_t attr, const uint32_t nl[3], float *leafRanges,
+                              cudaStream_t stream);
 // 16^3-voxel macrocell intervals (k_macrocell.cu): the volume check (throws
 // for volumes the legacy iterator does not cover), the number of
 // macrocells, their value ranges (2 floats each) and the batched walk.

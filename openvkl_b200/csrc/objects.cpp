@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <unordered_set>
 
 #include "kernels.h"
@@ -488,9 +489,6 @@ void Volume::commit()
   // node only with a non-constant node.temporalFormat (checked in
   // commitVdb).  The reference's VdbVolumeBuffers utility sets the node.*
   // temporal arrays on every volume it creates.
-  if (isDense && (getInt("temporallyStructuredNumTimesteps", 0) > 0 || getData("temporallyUnstructuredIndices")))
-    fail("temporally varying (motion blur) volumes are not supported by the cuda device",
-         VKL_INVALID_OPERATION);
   if (isDense)
     commitDense();
   else
@@ -521,6 +519,68 @@ void Volume::finishCommit(const float lo[3], const float hi[3])
   bounds = {{b[0], b[1], b[2]}, {b[3], b[4], b[5]}};
 }
 
+// verifyTemporalData (common/temporal_data_verification.h:10-181): the
+// reference's checks and messages; returns the number of data elements the
+// temporal format implies.
+uint64_t verifyTemporalData(uint64_t numVoxels, uint32_t format, int numTimesteps, Data *indices, Data *times)
+{
+  if (format == 0) {
+    if (numTimesteps != 0)
+      fail("Temporally constant volumes should not have temporallyStructuredNumTimesteps provided");
+    if (indices || times)
+      fail("Temporally constant volumes should not have temporallyUnstructuredIndices or "
+           "temporallyUnstructuredTimes provided");
+    return numVoxels;
+  }
+  if (format == 1) {
+    if (indices || times)
+      fail("Temporally structured volumes should not have temporallyUnstructuredIndices or "
+           "temporallyUnstructuredTimes provided");
+    return numVoxels * (uint64_t)numTimesteps;
+  }
+  if (numTimesteps != 0)
+    fail("Temporally unstructured volumes should not have temporallyStructuredNumTimesteps provided");
+  if (!times)
+    fail("temporal format is VKL_TEMPORAL_FORMAT_UNSTRUCTURED but temporallyUnstructuredTimes is not "
+         "specified.");
+  if (indices->numItems < numVoxels + 1)
+    fail("temporallyUnstructuredIndices is too small.");
+  const bool need64 = numVoxels >= (uint64_t)std::numeric_limits<uint32_t>::max();
+  if (need64 && indices->type != VKL_ULONG)
+    fail("temporallyUnstructuredIndices must be VKL_ULONG due to attribute data size");
+  if (indices->type != VKL_UINT && indices->type != VKL_ULONG)
+    fail("temporallyUnstructuredIndices must have type VKL_UINT or VKL_ULONG");
+  if (times->type != VKL_FLOAT)
+    fail("temporallyUnstructuredIndices must have type VKL_FLOAT");
+  const uint8_t *ib = indices->hostBytes();
+  const float *t    = (const float *)times->hostBytes();
+  auto at           = [&](uint64_t i) -> uint64_t {
+    if (indices->type == VKL_ULONG) {
+      uint64_t v;
+      std::memcpy(&v, ib + 8 * i, 8);
+      return v;
+    }
+    uint32_t v;
+    std::memcpy(&v, ib + 4 * i, 4);
+    return v;
+  };
+  uint64_t b = 0, e = 0;
+  for (uint64_t i = 0; i < numVoxels; ++i) {
+    b = at(i);
+    e = at(i + 1);
+    if (!(b < e))
+      fail("temporallyUnstructuredIndices must increase strictly monotonically.");
+    if (!(e <= times->numItems))
+      fail("Values in temporallyUnstructuredIndices are out of bounds in temporallyUnstructredTimes.");
+    for (uint64_t k = b + 1; k < e; ++k)
+      if (!(t[k - 1] < t[k]))
+        fail("temporallyUnstructuredTimes must increase strictly monotonically for every voxel.");
+    if (t[b] < 0.f || t[b] > 1.f || t[e - 1] < 0.f || t[e - 1] > 1.f)
+      fail("Values in temporallyUnstructuredTimes must be bounded by 0.0 and 1.0 for every voxel.");
+  }
+  return e;
+}
+
 void Volume::commitDense()
 {
   const int zero3[3] = {0, 0, 0};
@@ -542,14 +602,22 @@ void Volume::commitDense()
   if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0)
     fail("Vdb volumes must have at least one leaf node.");
   const uint64_t nvox = (uint64_t)dims[0] * dims[1] * dims[2];
-  for (size_t i = 0; i < attrs.size(); ++i) {
+  for (size_t i = 0; i < attrs.size(); ++i)
     if (!isVoxelType(attrs[i]->type))
       fail("structuredRegular: unsupported data element type (attribute " + std::to_string(i) +
                ") for 'data' parameter");
-    if (attrs[i]->numItems != nvox)
+  // Motion-blur data (DenseVdbVolume.cpp:149-186): the temporal format
+  // follows from which parameters are present, and the data arrays must
+  // hold the number of elements it implies.
+  const int numTimesteps = getInt("temporallyStructuredNumTimesteps", 0);
+  Data *tIdx             = getData("temporallyUnstructuredIndices");
+  Data *tTimes           = getData("temporallyUnstructuredTimes");
+  const uint32_t temporal = numTimesteps > 0 ? 1u : (tIdx ? 2u : 0u);
+  const uint64_t expectedItems = verifyTemporalData(nvox, temporal, numTimesteps, tIdx, tTimes);
+  for (size_t i = 0; i < attrs.size(); ++i)
+    if (attrs[i]->numItems != expectedItems)
       fail("attribute " + std::to_string(i) + " has " + std::to_string(attrs[i]->numItems) +
-               " elements, but expected " + std::to_string(nvox));
-  }
+               " elements, but expected " + std::to_string(expectedItems));
 
   grid.dense            = 1;
   grid.constantCellData = getBool("cellCentered", false) ? 1 : 0;
@@ -629,6 +697,40 @@ void Volume::commitDense()
   DeviceBuffer &leafRanges = *newBuffer(grid.numLeaves * 8), &volRange = *newBuffer(12 * NA);
   uint32_t *denormalFlags  = (uint32_t *)(volRange.as<float>() + 2 * NA);
   cudaCheck(cudaMemsetAsync(denormalFlags, 0, 4 * NA, st), "memset");
+  if (temporal) {
+    // the data stay as given (x fastest, time samples consecutive): no
+    // bricked copy and no texture atlas
+    grid.temporal     = temporal;
+    grid.numTimesteps = (uint32_t)std::max(numTimesteps, 0);
+    if (temporal == 2) {
+      keep.emplace_back(tIdx);
+      keep.emplace_back(tTimes);
+      grid.tIndices = tIdx->dev;
+      grid.tIndex64 = tIdx->type == VKL_ULONG ? 1u : 0u;
+      grid.tTimes   = (const float *)tTimes->dev;
+    }
+    for (uint32_t a = 0; a < NA; ++a) {
+      keep.emplace_back(attrs[a]);
+      grid.data[a] = attrs[a]->dev;
+      grid.type[a] = attrs[a]->type;
+      if (atlases[a])
+        device->giveAtlas(std::move(atlases[a]));
+      launchTemporalLeafRanges(grid, a, nl, leafRanges.as<float>(), st);
+      launchPropagateRanges(grid, a, grid.numLeaves, nullptr, leafRanges.as<float>(),
+                            volRange.as<float>() + 2 * a, nl, st);
+    }
+    std::vector<float> vr(3 * NA);
+    cudaCheck(cudaMemcpyAsync(vr.data(), volRange.ptr, 12 * NA, cudaMemcpyDeviceToHost, st),
+              "value range readback");
+    cudaCheck(cudaStreamSynchronize(st), "dense commit");
+    rangeLo.assign(NA, 0);
+    rangeHi.assign(NA, 0);
+    for (uint32_t a = 0; a < NA; ++a) {
+      rangeLo[a] = vr[2 * a];
+      rangeHi[a] = vr[2 * a + 1];
+    }
+    return;
+  }
   const uint32_t udims[3] = {(uint32_t)dims[0], (uint32_t)dims[1], (uint32_t)dims[2]};
   const uint64_t nb       = brickedElements(udims, grid.superX, grid.superY);
   // Texture atlases of float attributes (trilinear sampling through tld4):

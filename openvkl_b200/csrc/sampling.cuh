@@ -212,6 +212,115 @@ struct DenseField {
 };
 
 // ---------------------------------------------------------------------------
+// Temporally varying dense data (motion blur): every tap is the voxel's
+// value interpolated at the sample's time, then the spatial filter runs on
+// those values as on constant data (the reference's dense structured /
+// unstructured handlers, VdbSampler_dense.ih:347-500, with
+// temporal_data_interpolation.ih:22-190).  The voxel arrays are x fastest
+// with each voxel's time samples consecutive.  Times outside [0, 1] (which
+// the reference asserts against in debug builds) are clamped into it.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct TemporalDenseField {
+  const T *data;
+  uint32_t ax, ay, az;
+  int32_t rx, ry, rz;
+  float bg;
+  uint32_t format, N, idx64;
+  const void *idx;
+  const float *times;
+  float time;
+
+  __device__ __forceinline__ TemporalDenseField(const DevGrid &g, uint32_t a, float t)
+      : data((const T *)g.data[a]),
+        ax(g.activeSize[0]),
+        ay(g.activeSize[1]),
+        az(g.activeSize[2]),
+        rx(g.rootOrigin[0]),
+        ry(g.rootOrigin[1]),
+        rz(g.rootOrigin[2]),
+        bg(g.background[a]),
+        format(g.temporal),
+        N(g.numTimesteps),
+        idx64(g.tIndex64),
+        idx(g.tIndices),
+        times(g.tTimes),
+        time(fminf(fmaxf(t, 0.f), 1.f))
+  {
+  }
+
+  __device__ __forceinline__ uint64_t index(uint64_t v) const
+  {
+    return idx64 ? __ldg((const unsigned long long *)idx + v) : (uint64_t)__ldg((const uint32_t *)idx + v);
+  }
+
+  // one voxel's value at `time`
+  __device__ __forceinline__ float voxel(uint64_t v) const
+  {
+    if (format == 1) {
+      const float tf      = time * ((float)(N - 1));
+      const uint32_t ts   = (uint32_t)tf;
+      const float w       = tf - (float)ts;
+      const uint32_t next = (w == 0.f) ? ts : ts + 1;
+      const uint64_t base = (uint64_t)N * v;
+      return (1.f - w) * ldv(data, base + ts) + w * ldv(data, base + next);
+    }
+    const uint64_t b = index(v), e = index(v + 1);
+    const float t0   = __ldg(times + b);
+    if (time <= t0)
+      return ldv(data, b);
+    const float t1 = __ldg(times + e - 1);
+    if (time >= t1)
+      return ldv(data, e - 1);
+    if (e - b == 2) {
+      const float w = (time - t0) * (1.f / (t1 - t0));
+      return (1.f - w) * ldv(data, b) + w * ldv(data, e - 1);
+    }
+    // binary search for the bracketing samples (at most 64 halvings: the
+    // loop cannot run on when a time is out of order)
+    uint64_t lower = 0, upper = e - b;
+    for (int it = 0; it < 64 && lower <= upper; ++it) {
+      const uint64_t mid = (lower + upper) / 2;
+      const float tm     = __ldg(times + b + mid);
+      if (time >= tm && time <= __ldg(times + b + mid + 1)) {
+        lower = b + mid;
+        upper = lower + 1;
+        break;
+      } else if (time < tm) {
+        upper = mid;
+      } else {
+        lower = mid;
+      }
+    }
+    const float tl = __ldg(times + lower), th = __ldg(times + upper);
+    const float w  = (time - tl) * (1.f / (th - tl));
+    return (1.f - w) * ldv(data, lower) + w * ldv(data, upper);
+  }
+
+  __device__ __forceinline__ float at(int32_t x, int32_t y, int32_t z) const
+  {
+    const uint32_t ox = (uint32_t)(x - rx), oy = (uint32_t)(y - ry), oz = (uint32_t)(z - rz);
+    if (ox < ax && oy < ay && oz < az)
+      return voxel((uint64_t)ox + (uint64_t)ax * ((uint64_t)oy + (uint64_t)ay * (uint64_t)oz));
+    return bg;
+  }
+
+  __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
+  {
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      s[c] = at(x + (c >> 2), y + ((c >> 1) & 1), z + (c & 1));
+  }
+
+  __device__ __forceinline__ void stencil64(int32_t x, int32_t y, int32_t z, float s[64]) const
+  {
+#pragma unroll 4
+    for (int c = 0; c < 64; ++c)
+      s[c] = at(x - 1 + (c >> 4), y - 1 + ((c >> 2) & 3), z - 1 + (c & 3));
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Dense float attribute read through its z-plane texture atlas (DevGrid::
 // atlasTex): the 8 trilinear corners are two tld4 footprint gathers, one per
 // z-plane, instead of 8 loads through the L1 load/store pipe.  Point
@@ -659,11 +768,33 @@ __device__ __forceinline__ float sampleFiltered(const Field &F, int filter, bool
 // Sample at an object-space point with runtime type dispatch (used by the
 // hit iterator's marching, VdbSampler_iterator_computeSample_varying,
 // VdbSampler.ispc:341-374).
+// Temporally varying dense data: F is TemporalDenseField<T> at `time`.
+template <class Fn>
+__device__ __forceinline__ auto withTemporalField(const DevGrid &g, uint32_t attr, float time, Fn &&fn)
+{
+  switch (g.type[attr]) {
+  case kUChar:
+    return fn(TemporalDenseField<uint8_t>(g, attr, time));
+  case kShort:
+    return fn(TemporalDenseField<int16_t>(g, attr, time));
+  case kUShort:
+    return fn(TemporalDenseField<uint16_t>(g, attr, time));
+  case kHalf:
+    return fn(TemporalDenseField<__half>(g, attr, time));
+  case kDouble:
+    return fn(TemporalDenseField<double>(g, attr, time));
+  default:
+    return fn(TemporalDenseField<float>(g, attr, time));
+  }
+}
+
 __device__ __forceinline__ float sampleIndexAny(const DevGrid &g, int filter, uint32_t attr,
-                                                uint32_t depth, f3 p)
+                                                uint32_t depth, f3 p, float time = 0.f)
 {
   const bool cc = g.constantCellData != 0;
   const uint32_t t = g.type[attr];
+  if (g.temporal)
+    return withTemporalField(g, attr, time, [&](const auto &F) { return sampleFiltered(F, filter, cc, p); });
   if (g.dense) {
     switch (t) {
     case kUChar:
@@ -707,10 +838,13 @@ __device__ __forceinline__ f3 gradientFiltered(const DevGrid &g, const Field &F,
   return xfmNormal(g.objectToIndex, gi);
 }
 
-__device__ __forceinline__ f3 gradientObjectAny(const DevGrid &g, int filter, uint32_t attr, uint32_t depth, f3 oc)
+__device__ __forceinline__ f3 gradientObjectAny(const DevGrid &g, int filter, uint32_t attr, uint32_t depth, f3 oc,
+                                                float time = 0.f)
 {
   const f3 p       = xfmPoint(g.objectToIndex, oc);
   const uint32_t t = g.type[attr];
+  if (g.temporal)
+    return withTemporalField(g, attr, time, [&](const auto &F) { return gradientFiltered(g, F, filter, p); });
   if (g.dense) {
     switch (t) {
     case kUChar:
@@ -743,9 +877,9 @@ __device__ __forceinline__ f3 gradientObjectAny(const DevGrid &g, int filter, ui
 }
 
 __device__ __forceinline__ float sampleObjectAny(const DevGrid &g, int filter, uint32_t attr,
-                                                 uint32_t depth, f3 oc)
+                                                 uint32_t depth, f3 oc, float time = 0.f)
 {
-  return sampleIndexAny(g, filter, attr, depth, xfmPoint(g.objectToIndex, oc));
+  return sampleIndexAny(g, filter, attr, depth, xfmPoint(g.objectToIndex, oc), time);
 }
 
 }  // namespace vklcuda

@@ -27,6 +27,7 @@ VKL_STRING = 1500
 VKL_UCHAR, VKL_SHORT, VKL_USHORT = 2500, 3000, 3500
 VKL_INT, VKL_VEC3I = 4000, 4002
 VKL_UINT = 4500
+VKL_ULONG = 5550
 VKL_HALF, VKL_FLOAT, VKL_VEC3F, VKL_DOUBLE = 5800, 6000, 6002, 7000
 VKL_BOX1F, VKL_BOX3I = 10000, 8002
 VKL_AFFINE3F = 12003
@@ -43,9 +44,10 @@ _NP2VKL = {
     np.dtype(np.float64): VKL_DOUBLE,
     np.dtype(np.int32): VKL_INT,
     np.dtype(np.uint32): VKL_UINT,
+    np.dtype(np.uint64): VKL_ULONG,
 }
 _VKL_ITEM = {VKL_UCHAR: 1, VKL_SHORT: 2, VKL_USHORT: 2, VKL_HALF: 2, VKL_FLOAT: 4,
-             VKL_DOUBLE: 8, VKL_INT: 4, VKL_UINT: 4, VKL_VEC3I: 12, VKL_VEC3F: 12, VKL_BOX1F: 8}
+             VKL_DOUBLE: 8, VKL_INT: 4, VKL_UINT: 4, VKL_ULONG: 8, VKL_VEC3I: 12, VKL_VEC3F: 12, VKL_BOX1F: 8}
 
 # Exported symbols declared in include/openvkl_cuda.h.
 EXPORTS = [
@@ -240,6 +242,21 @@ def _ptr(a):
         assert a.is_contiguous()
         return a.data_ptr()
     return a.ctypes.data
+
+
+def _times(times):
+    """Pointer to a per-point time array (None -> NULL); numpy arrays are
+    made contiguous float32 and must stay alive for the call."""
+    if times is None:
+        return None
+    if _is_torch(times):
+        return C.c_void_p(times.data_ptr())
+    global _times_keep
+    _times_keep = np.ascontiguousarray(times, np.float32)
+    return C.c_void_p(_times_keep.ctypes.data)
+
+
+_times_keep = None
 
 
 def _alloc_like(ref, shape, dtype=np.float32):
@@ -460,13 +477,25 @@ class VKLObserverObj(_Obj):
 
 def structured_regular(device: Device, data, grid_origin=None, grid_spacing=None, cell_centered=False,
                        index_to_object=None, index_origin=None, background=None, filter=None,
-                       shared=False):
+                       shared=False, dims=None, num_timesteps=None, time_indices=None, times=None):
     """A committed structuredRegular volume; `data` is one array or a list
-    (one per attribute), each shaped (Z, Y, X) with x fastest."""
+    (one per attribute), each shaped (Z, Y, X) with x fastest.  Temporally
+    varying data: `dims` = (X, Y, Z) and flat data arrays with each voxel's
+    time samples consecutive, plus `num_timesteps` (structured) or
+    `time_indices` (uint32 / uint64, one per voxel + 1) and `times`
+    (unstructured)."""
     arrays = data if isinstance(data, (list, tuple)) else [data]
-    shape = tuple(arrays[0].shape)
+    shape = tuple(arrays[0].shape) if dims is None else tuple(dims)[::-1]
     v = Volume(device, "structuredRegular")
     v.set_vec3i("dimensions", shape[::-1])
+    if num_timesteps is not None:
+        v.set_int("temporallyStructuredNumTimesteps", num_timesteps)
+    if time_indices is not None:
+        idx = np.ascontiguousarray(time_indices)
+        v.set_data("temporallyUnstructuredIndices",
+                   Data(device, idx, vkl_type=VKL_ULONG if idx.dtype == np.uint64 else VKL_UINT))
+    if times is not None:
+        v.set_data("temporallyUnstructuredTimes", Data(device, np.ascontiguousarray(times, np.float32)))
     if grid_origin is not None:
         v.set_vec3f("gridOrigin", grid_origin)
     if grid_spacing is not None:
@@ -697,36 +726,39 @@ class Sampler(_Obj):
         self.device.raise_pending()
         return VKLObserverObj(self.device, h, "vklNewSamplerObserver")
 
-    def sample(self, points, attr=0, out=None):
+    def sample(self, points, attr=0, out=None, times=None):
+        """vklComputeSampleN; `times`: one time per point (temporally varying
+        volumes), host or device array, or None."""
         n = points.shape[0]
         if out is None:
             out = _alloc_like(points, (n,))
-        self._call(self.lib.vklComputeSampleN, C.byref(self.h), n, _ptr(points), _ptr(out), attr, None)
+        self._call(self.lib.vklComputeSampleN, C.byref(self.h), n, _ptr(points), _ptr(out), attr, _times(times))
         return out
 
-    def sample_m(self, points, attrs, out=None):
+    def sample_m(self, points, attrs, out=None, times=None):
         n = points.shape[0]
         a = np.ascontiguousarray(attrs, np.uint32)
         if out is None:
             out = _alloc_like(points, (n, len(a)))
         self._call(self.lib.vklComputeSampleMN, C.byref(self.h), n, _ptr(points), _ptr(out), len(a),
-                   a.ctypes.data, None)
+                   a.ctypes.data, _times(times))
         return out
 
-    def gradient(self, points, attr=0, out=None):
+    def gradient(self, points, attr=0, out=None, times=None):
         n = points.shape[0]
         if out is None:
             out = _alloc_like(points, (n, 3))
-        self._call(self.lib.vklComputeGradientN, C.byref(self.h), n, _ptr(points), _ptr(out), attr, None)
+        self._call(self.lib.vklComputeGradientN, C.byref(self.h), n, _ptr(points), _ptr(out), attr,
+                   _times(times))
         return out
 
-    def sample_one(self, p, attr=0):
+    def sample_one(self, p, attr=0, time=0.0):
         v = vec3f(*[float(x) for x in p])
-        return self._call(self.lib.vklComputeSample, C.byref(self.h), C.byref(v), attr, 0.0)
+        return self._call(self.lib.vklComputeSample, C.byref(self.h), C.byref(v), attr, float(time))
 
-    def gradient_one(self, p, attr=0):
+    def gradient_one(self, p, attr=0, time=0.0):
         v = vec3f(*[float(x) for x in p])
-        g = self._call(self.lib.vklComputeGradient, C.byref(self.h), C.byref(v), attr, 0.0)
+        g = self._call(self.lib.vklComputeGradient, C.byref(self.h), C.byref(v), attr, float(time))
         return np.array([g.x, g.y, g.z], np.float32)
 
     def sample_w(self, points, valid=None, attr=0):

@@ -89,6 +89,12 @@ def lib(fast: bool = False, fma: bool = False) -> C.CDLL:
         L.orc_sample_parallel.argtypes = [P, C.c_int, U64, P, U32, P, C.c_int]
         L.orc_gradient_parallel.argtypes = [P, C.c_int, U32, U64, P, U32, P, C.c_int]
         L.orc_macrocell_ranges.argtypes = [P, U32, P]
+        L.orc_dense_create_temporal.restype = P
+        L.orc_dense_create_temporal.argtypes = [P, U32, P, P, P, C.c_int, P, P, P, P, C.c_int, P, U32, U64, P,
+                                                U64]
+        L.orc_sample_times.argtypes = [P, C.c_int, U64, P, P, U32, P, C.c_int]
+        L.orc_path_trace.argtypes = [P, C.c_int, U32, U32, P, P, C.c_int, P, C.c_int, C.c_int, P, P, P, P, P]
+        L.orc_gradient_times.argtypes = [P, C.c_int, U64, P, P, U32, P, C.c_int]
         L.orc_iterate_macrocells.restype = C.c_int
         L.orc_iterate_macrocells.argtypes = [P, U32, U32, P, U64, P, P, P, U32, P, P]
         L.orc_sample_observed.argtypes = [P, C.c_int, U32, U64, P, U32, P, P]
@@ -152,6 +158,36 @@ class OracleVolume:
         if not h:
             raise RuntimeError(L.orc_last_error().decode())
         return OracleVolume(h, {"arrays": arrays, "dense": True}, fast, fma)
+
+    @staticmethod
+    def dense_temporal(data, dims, num_timesteps=0, indices=None, times=None, cell_centered=False,
+                       grid_origin=None, grid_spacing=None, index_to_object=None, background=None, fast=False,
+                       fma=False):
+        """A structuredRegular volume with temporally varying data: `data` is
+        one flat array per attribute (x-fastest voxels, each voxel's time
+        samples consecutive), `dims` = (X, Y, Z); structured with
+        num_timesteps > 0, unstructured with per-voxel `indices` (uint32 /
+        uint64, X*Y*Z + 1 entries) into data and `times`."""
+        arrays = data if isinstance(data, (list, tuple)) else [data]
+        arrays = [np.ascontiguousarray(a).reshape(-1) for a in arrays]
+        d = np.array(dims, np.int32)
+        ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+        types = np.array([_NP2VKL[a.dtype] for a in arrays], np.uint32)
+        items = np.array([a.size for a in arrays], np.uint64)
+        idx = None if indices is None else np.ascontiguousarray(indices)
+        itype = 0 if idx is None else (5550 if idx.dtype == np.uint64 else 4500)
+        tm = None if times is None else np.ascontiguousarray(times, np.float32)
+        go = None if grid_origin is None else np.asarray(grid_origin, np.float32)
+        gs = None if grid_spacing is None else np.asarray(grid_spacing, np.float32)
+        i2o = None if index_to_object is None else np.asarray(index_to_object, np.float32)
+        bg = None if background is None else np.asarray(background, np.float32).reshape(-1)
+        L = lib(fast, fma)
+        h = L.orc_dense_create_temporal(_p(d), len(arrays), ptrs, _p(types), _p(items), int(bool(cell_centered)),
+                                        _p(go), _p(gs), _p(i2o), _p(bg), int(num_timesteps), _p(idx), itype,
+                                        0 if idx is None else idx.size, _p(tm), 0 if tm is None else tm.size)
+        if not h:
+            raise RuntimeError(L.orc_last_error().decode())
+        return OracleVolume(h, {"arrays": arrays, "idx": idx, "times": tm, "dense": True}, fast, fma)
 
     @staticmethod
     def vdb_volume(levels, origins, formats, packed_dense, packed_tile=None,
@@ -243,6 +279,20 @@ class OracleVolume:
                                         threads)
         return out
 
+    def sample_times(self, points, times, filter=FILTER_LINEAR, attr=0, threads=0):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        t = None if times is None else np.ascontiguousarray(times, np.float32).reshape(-1)
+        out = np.zeros(len(pts), np.float32)
+        self._lib.orc_sample_times(self._h, filter, len(pts), _p(pts), _p(t), attr, _p(out), threads)
+        return out
+
+    def gradient_times(self, points, times, filter=FILTER_LINEAR, attr=0, threads=0):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        t = None if times is None else np.ascontiguousarray(times, np.float32).reshape(-1)
+        out = np.zeros((len(pts), 3), np.float32)
+        self._lib.orc_gradient_times(self._h, filter, len(pts), _p(pts), _p(t), attr, _p(out), threads)
+        return out
+
     def sample_fp64(self, points, filter=FILTER_LINEAR, attr=0):
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         out = np.zeros(len(pts), np.float64)
@@ -313,6 +363,25 @@ class OracleVolume:
                              max_sampling_depth, attr, 0 if vr is None else len(vr), _p(vr), hint, len(iso),
                              _p(iso), _p(cam), _p(tfc), len(tfc), _p(tfr), _p(ip), _p(fp), _p(out))
         return out
+
+    def path_trace(self, camera, tf_colors, tf_range, width, height, bounds, frames=(0,), filter=FILTER_LINEAR,
+                   max_sampling_depth=3, attr=0, time=0.0, shutter=0.0, motion_blur=False, sigma_t_scale=1.0,
+                   sigma_s_scale=1.0, max_num_scatters=1, ambient_light_intensity=1.0, show_bbox=False):
+        """The density path tracer restated (orc_path_trace): the frames'
+        contributions accumulated as the renderer does; returns (rgba
+        (H, W, 4), weights (H, W))."""
+        cam = np.ascontiguousarray(camera, np.float32).reshape(14)
+        tfc = np.ascontiguousarray(tf_colors, np.float32).reshape(-1, 4)
+        tfr = np.ascontiguousarray(tf_range, np.float32).reshape(2)
+        b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+        rgba = np.zeros((height, width, 4), np.float32)
+        w = np.zeros((height, width), np.float32)
+        for f in frames:
+            pt = np.array([shutter, sigma_t_scale, sigma_s_scale, ambient_light_intensity, time], np.float32)
+            ipt = np.array([int(motion_blur), max_num_scatters, int(show_bbox), f], np.int32)
+            self._lib.orc_path_trace(self._h, filter, max_sampling_depth, attr, _p(cam), _p(tfc), len(tfc), _p(tfr),
+                                     width, height, _p(b), _p(pt), _p(ipt), _p(rgba), _p(w))
+        return rgba, w
 
     def inner_nodes(self, max_depth=1, attr=0):
         n = int(self._lib.orc_inner_nodes(self._h, max_depth, attr, 0, None))

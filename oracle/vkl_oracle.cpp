@@ -17,6 +17,10 @@
 #include <atomic>
 #include <thread>
 
+// The density path tracer's log / sincos: the one source the CUDA renderer
+// compiles too (the reference's platform math differs between platforms).
+#include "../openvkl_b200/renderers/pt_math.h"
+
 namespace orc {
 
 static thread_local std::string g_lastError;
@@ -256,6 +260,14 @@ struct Grid {
   // indexToObject or indexOrigin (what the legacy macrocell iterator reads)
   bool legacyGrid = false;
   float gridOrigin[3] = {0, 0, 0}, gridSpacing[3] = {1, 1, 1};
+  // temporally varying dense data (0 constant, 1 structured: numTimesteps
+  // values per voxel; 2 unstructured: per-voxel [indices[v], indices[v+1])
+  // into the data and times arrays)
+  int temporalFormat = 0;
+  int numTimesteps   = 0;
+  const uint8_t *tIndices = nullptr;
+  bool tIndices64         = false;
+  const float *tTimes     = nullptr;
   std::vector<Attr> denseAttr;
   std::vector<std::vector<uint8_t>> denseCopies;
   // sparse packed
@@ -340,11 +352,80 @@ inline vec3ui toDomainOffset(const vec3i &ic, const vec3i &root)
           (uint32_t)(ic.z - root.z)};
 }
 
-// Dense voxel load (VdbSampler_dense.ih:282-345): x fastest, 64-bit index.
+// Time of the sample being computed on this thread (the `time` argument of
+// the sampling calls; temporally constant data ignore it).
+static thread_local float t_time = 0.f;
+
+inline uint64_t tIndex(const Grid &g, uint64_t v)
+{
+  if (g.tIndices64) {
+    uint64_t r;
+    std::memcpy(&r, g.tIndices + 8 * v, 8);
+    return r;
+  }
+  uint32_t r;
+  std::memcpy(&r, g.tIndices + 4 * v, 4);
+  return r;
+}
+
+// interpolateTemporallyStructured (temporal_data_interpolation.ih:22-55):
+// N values per voxel, regularly placed in [0, 1].
+inline float temporalStructured(const Attr &at, int N, uint64_t base, float time)
+{
+  const float tf        = time * ((float)(N - 1));
+  const uint32_t ts     = (uint32_t)tf;
+  const float w         = tf - (float)ts;
+  const uint32_t next   = (w == 0.f) ? ts : ts + 1;
+  const float v0 = loadAttr(at, base + ts), v1 = loadAttr(at, base + next);
+  return (1.f - w) * v0 + w * v1;
+}
+
+// interpolateTemporallyUnstructured (temporal_data_interpolation.ih:
+// 117-190): per-voxel times, clamped at both ends, binary search between.
+inline float temporalUnstructured(const Grid &g, const Attr &at, uint64_t voxel, float time)
+{
+  const uint64_t b = tIndex(g, voxel), e = tIndex(g, voxel + 1);
+  const float t0 = g.tTimes[b];
+  if (time <= t0)
+    return loadAttr(at, b);
+  const float t1 = g.tTimes[e - 1];
+  if (time >= t1)
+    return loadAttr(at, e - 1);
+  const uint64_t n = e - b;
+  if (n == 2) {
+    const float w = (time - t0) * (1.f / (t1 - t0));
+    return (1.f - w) * loadAttr(at, b) + w * loadAttr(at, e - 1);
+  }
+  uint64_t lower = 0, upper = n;
+  while (lower <= upper) {
+    const uint64_t mid = (lower + upper) / 2;
+    const float tm     = g.tTimes[b + mid];
+    if (time >= tm && time <= g.tTimes[b + mid + 1]) {
+      lower = b + mid;
+      upper = lower + 1;
+      break;
+    } else if (time < tm) {
+      upper = mid;
+    } else {
+      lower = mid;
+    }
+  }
+  const float tl = g.tTimes[lower], th = g.tTimes[upper];
+  const float w  = (time - tl) * (1.f / (th - tl));
+  return (1.f - w) * loadAttr(at, lower) + w * loadAttr(at, upper);
+}
+
+// Dense voxel load (VdbSampler_dense.ih:282-345): x fastest, 64-bit index;
+// temporally varying data interpolated at the thread's sample time (the
+// structured / unstructured handlers, VdbSampler_dense.ih:347-500).
 inline float denseLoad(const Grid &g, uint32_t a, const vec3ui &o)
 {
   const uint64_t idx = (uint64_t)o.z * g.activeSize.y * (uint64_t)g.activeSize.x +
                        (uint64_t)o.y * (uint64_t)g.activeSize.x + (uint64_t)o.x;
+  if (g.temporalFormat == 1)
+    return temporalStructured(g.denseAttr[a], g.numTimesteps, (uint64_t)g.numTimesteps * idx, t_time);
+  if (g.temporalFormat == 2)
+    return temporalUnstructured(g, g.denseAttr[a], idx, t_time);
   return loadAttr(g.denseAttr[a], idx);
 }
 
@@ -679,9 +760,31 @@ static range1f nodeValueRange(const Grid &g,
           if (!(o.x < (uint32_t)g.denseDims.x && o.y < (uint32_t)g.denseDims.y &&
                 o.z < (uint32_t)g.denseDims.z))
             continue;
-          const float v = denseLoad(g, a, o);
-          r.lower       = fmin_(r.lower, v);
-          r.upper       = fmax_(r.upper, v);
+          const uint64_t idx = (uint64_t)o.z * g.activeSize.y * (uint64_t)g.activeSize.x +
+                               (uint64_t)o.y * (uint64_t)g.activeSize.x + (uint64_t)o.x;
+          if (g.temporalFormat == 1) {
+            // every time step (VdbSampler_dense.ih:107-175)
+            for (int t = 0; t < g.numTimesteps; ++t) {
+              const float v = loadAttr(g.denseAttr[a], (uint64_t)g.numTimesteps * idx + t);
+              r.lower       = fmin_(r.lower, v);
+              r.upper       = fmax_(r.upper, v);
+            }
+          } else if (g.temporalFormat == 2) {
+            // the voxel's own range, then box_extend (VdbSampler_dense.ih:
+            // 177-266, temporal_data_interpolation.ih:226-260)
+            range1f vr;
+            for (uint64_t i = tIndex(g, idx); i < tIndex(g, idx + 1); ++i) {
+              const float v = loadAttr(g.denseAttr[a], i);
+              vr.lower      = fmin_(vr.lower, v);
+              vr.upper      = fmax_(vr.upper, v);
+            }
+            r.lower = fmin_(r.lower, vr.lower);
+            r.upper = fmax_(r.upper, vr.upper);
+          } else {
+            const float v = denseLoad(g, a, o);
+            r.lower       = fmin_(r.lower, v);
+            r.upper       = fmax_(r.upper, v);
+          }
         }
     return r;
   }
@@ -1357,24 +1460,86 @@ extern "C" {
 
 const char *orc_last_error(void) { return g_lastError.c_str(); }
 
-OrcVolume *orc_dense_create(const int32_t dims[3], uint32_t numAttributes,
-                            const void *const *data, const uint32_t *types,
-                            const uint64_t *byteStrides, int cellCentered,
-                            const float gridOrigin[3], const float gridSpacing[3],
-                            const float *indexToObject, const int32_t indexOrigin[3],
-                            const float *background)
+struct TemporalArgs {
+  int numTimesteps;
+  const void *indices;
+  uint32_t indexType;
+  uint64_t numIndices;
+  const float *times;
+  uint64_t numTimes;
+  const uint64_t *numItems;  // per attribute
+};
+
+// verifyTemporalData (common/temporal_data_verification.h:10-181) for the
+// structured / unstructured cases, with the reference's messages.
+static void verifyTemporal(Grid &g, uint64_t numVoxels, const TemporalArgs &t, uint32_t numAttributes)
+{
+  uint64_t expected = numVoxels;
+  if (t.numTimesteps > 0) {
+    if (t.indices || t.times)
+      throw std::runtime_error("Temporally structured volumes should not have temporallyUnstructuredIndices or "
+                               "temporallyUnstructuredTimes provided");
+    g.temporalFormat = 1;
+    g.numTimesteps   = t.numTimesteps;
+    expected         = numVoxels * (uint64_t)t.numTimesteps;
+  } else if (t.indices) {
+    if (!t.times)
+      throw std::runtime_error("temporal format is VKL_TEMPORAL_FORMAT_UNSTRUCTURED but "
+                               "temporallyUnstructuredTimes is not specified.");
+    if (t.numIndices < numVoxels + 1)
+      throw std::runtime_error("temporallyUnstructuredIndices is too small.");
+    if (t.indexType != 4500 && t.indexType != 5550)
+      throw std::runtime_error("temporallyUnstructuredIndices must have type VKL_UINT or VKL_ULONG");
+    g.temporalFormat = 2;
+    g.tIndices       = (const uint8_t *)t.indices;
+    g.tIndices64     = t.indexType == 5550;
+    g.tTimes         = t.times;
+    uint64_t b = 0, e = 0;
+    for (uint64_t i = 0; i < numVoxels; ++i) {
+      b = tIndex(g, i);
+      e = tIndex(g, i + 1);
+      if (!(b < e))
+        throw std::runtime_error("temporallyUnstructuredIndices must increase strictly monotonically.");
+      if (!(e <= t.numTimes))
+        throw std::runtime_error(
+            "Values in temporallyUnstructuredIndices are out of bounds in temporallyUnstructredTimes.");
+      for (uint64_t k = b + 1; k < e; ++k)
+        if (!(t.times[k - 1] < t.times[k]))
+          throw std::runtime_error(
+              "temporallyUnstructuredTimes must increase strictly monotonically for every voxel.");
+      if (t.times[b] < 0.f || t.times[b] > 1.f || t.times[e - 1] < 0.f || t.times[e - 1] > 1.f)
+        throw std::runtime_error(
+            "Values in temporallyUnstructuredTimes must be bounded by 0.0 and 1.0 for every voxel.");
+    }
+    expected = e;
+  } else if (t.times) {
+    throw std::runtime_error("Temporally constant volumes should not have temporallyUnstructuredIndices or "
+                             "temporallyUnstructuredTimes provided");
+  }
+  for (uint32_t a = 0; a < numAttributes; ++a)
+    if (t.numItems && t.numItems[a] != expected)
+      throw std::runtime_error("attribute " + std::to_string(a) + " has " + std::to_string(t.numItems[a]) +
+                               " elements, but expected " + std::to_string(expected));
+}
+
+static OrcVolume *denseCreate(const int32_t dims[3], uint32_t numAttributes, const void *const *data,
+                              const uint32_t *types, const uint64_t *byteStrides, int cellCentered,
+                              const float gridOrigin[3], const float gridSpacing[3], const float *indexToObject,
+                              const int32_t indexOrigin[3], const float *background, const TemporalArgs *temporal)
 {
   try {
     OrcVolume *v = new OrcVolume();
     Grid &g      = v->g;
     g.dense      = true;
+    if (temporal)
+      verifyTemporal(g, (uint64_t)dims[0] * (uint64_t)dims[1] * (uint64_t)dims[2], *temporal, numAttributes);
     g.constantCellData = cellCentered != 0;
     g.numAttributes    = numAttributes;
     g.denseDims        = {dims[0], dims[1], dims[2]};
     for (uint32_t a = 0; a < numAttributes; ++a) {
       typeSize(types[a]);
       g.denseAttr.push_back({types[a], (const uint8_t *)data[a],
-                             byteStrides[a] ? byteStrides[a] : typeSize(types[a])});
+                             (byteStrides && byteStrides[a]) ? byteStrides[a] : typeSize(types[a])});
       g.background.push_back(bgOr(background, a));
     }
     // transforms (DenseVdbVolume.cpp:42-64)
@@ -1426,6 +1591,55 @@ OrcVolume *orc_dense_create(const int32_t dims[3], uint32_t numAttributes,
     g_lastError = ex.what();
     return nullptr;
   }
+}
+
+OrcVolume *orc_dense_create(const int32_t dims[3], uint32_t numAttributes,
+                            const void *const *data, const uint32_t *types,
+                            const uint64_t *byteStrides, int cellCentered,
+                            const float gridOrigin[3], const float gridSpacing[3],
+                            const float *indexToObject, const int32_t indexOrigin[3],
+                            const float *background)
+{
+  return denseCreate(dims, numAttributes, data, types, byteStrides, cellCentered, gridOrigin, gridSpacing,
+                     indexToObject, indexOrigin, background, nullptr);
+}
+
+OrcVolume *orc_dense_create_temporal(const int32_t dims[3], uint32_t numAttributes, const void *const *data,
+                                     const uint32_t *types, const uint64_t *numItems, int cellCentered,
+                                     const float gridOrigin[3], const float gridSpacing[3],
+                                     const float *indexToObject, const float *background, int numTimesteps,
+                                     const void *indices, uint32_t indexType, uint64_t numIndices,
+                                     const float *times, uint64_t numTimes)
+{
+  const TemporalArgs t{numTimesteps, indices, indexType, numIndices, times, numTimes, numItems};
+  return denseCreate(dims, numAttributes, data, types, nullptr, cellCentered, gridOrigin, gridSpacing,
+                     indexToObject, nullptr, background, &t);
+}
+
+void orc_sample_times(const OrcVolume *v, int filter, uint64_t n, const float *pts, const float *times,
+                      uint32_t attr, float *out, int threads)
+{
+  const Grid &g = v->g;
+  parallelFor((int64_t)n, threads, 4096, [&](int64_t i) {
+    t_time        = times ? times[i] : 0.f;
+    const vec3f p = xfmPoint(g.o2i, {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]});
+    out[i]        = sampleAt(g, filter, p, attr, NUM_LEVELS - 1);
+  });
+  t_time = 0.f;
+}
+
+void orc_gradient_times(const OrcVolume *v, int filter, uint64_t n, const float *pts, const float *times,
+                        uint32_t attr, float *out, int threads)
+{
+  const uint64_t chunks = (n + 4095) / 4096;
+  parallelFor((int64_t)chunks, threads, 1, [&](int64_t c) {
+    const uint64_t b = (uint64_t)c * 4096, e = std::min<uint64_t>(n, b + 4096);
+    for (uint64_t i = b; i < e; ++i) {
+      t_time = times ? times[i] : 0.f;
+      orc_gradient(v, filter, NUM_LEVELS - 1, 1, pts + 3 * i, attr, out + 3 * i);
+    }
+    t_time = 0.f;
+  });
 }
 
 OrcVolume *orc_vdb_create(uint64_t numLeaves, const uint32_t *levels, const int32_t *origins,
@@ -2191,6 +2405,143 @@ void orc_render(const OrcVolume *v, int renderer, int filter, int gradientFilter
     rgba[4 * idx + 1] = color.y;
     rgba[4 * idx + 2] = color.z;
     rgba[4 * idx + 3] = 1.f;
+  });
+}
+
+// The density path tracer (examples/interactive/renderer/density_path_tracer/
+// DensityPathTracerGpuKernel.cpp:9-170, RandomTEA of Random.ih): one
+// progressive frame added into rgba (4 floats per pixel) and weights.  The
+// camera ray passes through the pixel centre as in orc_render.  pt: shutter,
+// sigmaTScale, sigmaSScale, ambientLightIntensity, time; ipt: motionBlur,
+// maxNumScatters, showBbox, frame.
+void orc_path_trace(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint32_t attr,
+                    const float camera[14], const float *tfColors, int tfNum, const float tfRange[2], int W, int H,
+                    const float bounds[6], const float pt[5], const int ipt[4], float *rgba, float *weights)
+{
+  const Grid &g = v->g;
+  const RenderTF tf{tfColors, tfNum, tfRange[0], tfRange[1]};
+  const float shutter = pt[0], sigmaMax0 = pt[1], sigmaSScale = pt[2], ambient = pt[3], time0 = pt[4];
+  const bool motionBlur = ipt[0] != 0, showBbox = ipt[2] != 0;
+  const int maxNumScatters = ipt[1];
+  const uint32_t frame     = (uint32_t)ipt[3];
+  const float inf          = std::numeric_limits<float>::infinity();
+  struct Tea {
+    uint32_t v0, v1;
+    void floats(float &a, float &b)
+    {
+      uint32_t sum = 0;
+      for (int i = 0; i < 8; ++i) {
+        sum += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + sum) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + sum) ^ ((v0 >> 5) + 0x7e95761eu);
+      }
+      a = (float)v0 * 2.3283064365386962890625e-10f;
+      b = (float)v1 * 2.3283064365386962890625e-10f;
+    }
+  };
+  auto box = [&](RV3 org, RV3 dir) {
+    const float rx = 1.f / dir.x, ry = 1.f / dir.y, rz = 1.f / dir.z;
+    const float x0 = (bounds[0] - org.x) * rx, y0 = (bounds[1] - org.y) * ry, z0 = (bounds[2] - org.z) * rz;
+    const float x1 = (bounds[3] - org.x) * rx, y1 = (bounds[4] - org.y) * ry, z1 = (bounds[5] - org.z) * rz;
+    range1f tr;
+    tr.lower = std::fmax(std::fmax(std::fmax(std::fmin(x0, x1), std::fmin(y0, y1)), std::fmin(z0, z1)), 0.f);
+    tr.upper = std::fmin(std::fmin(std::fmin(std::fmax(x0, x1), std::fmax(y0, y1)), std::fmax(z0, z1)), inf);
+    return tr;
+  };
+  parallelFor((int64_t)W * H, 0, 16, [&](int64_t idx) {
+    const float px = (float)(idx % W) + 0.5f, py = (float)(idx / W) + 0.5f;
+    const float irx     = 1.f / (float)W;
+    const float sx      = (px - 0.5f * (float)W) * irx;
+    const float sy      = -(py - 0.5f * (float)H) * irx;
+    const RV3 pCamera   = {camera[0] * sx, camera[0] * sy, 0.f};
+    const RV3 pAperture = {0.f, 0.f, -camera[1]};
+    const RV3 dCamera   = pAperture - pCamera;
+    const RV3 R0 = {camera[2], camera[3], camera[4]}, R1 = {camera[5], camera[6], camera[7]},
+              R2 = {camera[8], camera[9], camera[10]};
+    RV3 org = {rdot(R0, pCamera) + camera[11], rdot(R1, pCamera) + camera[12], rdot(R2, pCamera) + camera[13]};
+    RV3 dir = rnormalize({rdot(R0, dCamera), rdot(R1, dCamera), rdot(R2, dCamera)});
+    Tea rng{frame, (uint32_t)idx};
+    int maxScatterIndex      = 0;
+    bool primaryRayIntersect = false;
+    RV3 Le = {0.f, 0.f, 0.f}, sigmaS = {0.f, 0.f, 0.f};
+    for (int scatterIndex = 0; true; scatterIndex++) {
+      float sample    = 0.f;
+      maxScatterIndex = std::max(scatterIndex, maxScatterIndex);
+      const range1f rt = box(org, dir);
+      const bool empty = rt.lower > rt.upper;
+      if (scatterIndex == 0 && !empty)
+        primaryRayIntersect = true;
+      if (empty)
+        break;
+      // sampleWoodcock
+      float t = rt.lower, transmittance = 0.f;
+      bool event = false;
+      if (sigmaMax0 <= 0.f) {
+        transmittance = 1.f;
+      } else {
+        for (int step = 0; step < (1 << 16); ++step) {
+          float r0, r1, s0, s1;
+          rng.floats(r0, r1);
+          rng.floats(s0, s1);
+          t = t + (-pt_log(1.f - r0)) / sigmaMax0;
+          if (t > rt.upper) {
+            transmittance = 1.f;
+            break;
+          }
+          const RV3 c = org + t * dir;
+          float time  = time0;
+          if (motionBlur)
+            time = time + (s0 - 0.5f) * shutter;
+          t_time      = std::fmin(std::fmax(time, 0.f), 1.f);
+          sample      = sampleAt(g, filter, xfmPoint(g.o2i, {c.x, c.y, c.z}), attr, maxSamplingDepth);
+          t_time      = 0.f;
+          float sc[4];
+          tf.at(sample, sc);
+          const float sigmaTSample = sigmaMax0 * sc[3];
+          if (r1 < sigmaTSample / sigmaMax0) {
+            event = true;
+            break;
+          }
+          if (step + 1 == (1 << 16))
+            event = true;
+        }
+        if (event)
+          transmittance = 0.f;
+      }
+      if (!event) {
+        if (scatterIndex > 0) {
+          const float a = transmittance * ambient;
+          Le            = Le + RV3{a * sigmaS.x, a * sigmaS.y, a * sigmaS.z};
+        }
+        break;
+      }
+      if (scatterIndex >= maxNumScatters)
+        break;
+      float sc[4];
+      tf.at(sample, sc);
+      sigmaS = {sigmaSScale * sc[0] * sc[3], sigmaSScale * sc[1] * sc[3], sigmaSScale * sc[2] * sc[3]};
+      org    = org + t * dir;
+      float s0, s1;
+      rng.floats(s0, s1);
+      const float phi      = 6.28318530717958647692f * s0;
+      const float cosTheta = 1.f * (1.f - 2.f * s1);
+      const float sinTheta = 2.f * 1.f * std::sqrt(s1 * (1.f - s1));
+      float sinPhi, cosPhi;
+      pt_sincos(phi, &sinPhi, &cosPhi);
+      dir = {cosPhi * sinTheta, sinPhi * sinTheta, cosTheta};
+    }
+    RV3 color   = Le;
+    float alpha = maxScatterIndex > 0 ? 1.f : 0.f;
+    if (showBbox && primaryRayIntersect) {
+      const float blend = 0.2f;
+      alpha             = (1.f - blend) * alpha + blend * 1.f;
+      color             = (1.f - blend) * color + RV3{blend * 1.f, blend * 1.f, blend * 1.f};
+    }
+    rgba[4 * idx]     = rgba[4 * idx] + color.x;
+    rgba[4 * idx + 1] = rgba[4 * idx + 1] + color.y;
+    rgba[4 * idx + 2] = rgba[4 * idx + 2] + color.z;
+    rgba[4 * idx + 3] = rgba[4 * idx + 3] + alpha;
+    weights[idx]      = weights[idx] + 1.f;
   });
 }
 

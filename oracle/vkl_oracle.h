@@ -119,6 +119,29 @@ void orc_macrocell_ranges(const OrcVolume *v, uint32_t attr, float *out);
 int orc_iterate_macrocells(const OrcVolume *v, uint32_t attr, uint32_t numRanges, const float *ranges,
                            uint64_t numRays, const float *origins, const float *directions,
                            const float *tRanges, uint32_t maxIntervals, float *out, uint32_t *counts);
+// A structuredRegular volume with temporally varying data (motion blur):
+// numTimesteps > 0 for structured data (numTimesteps values per voxel), or
+// per-voxel indices (VKL_UINT 4500 / VKL_ULONG 5550, numVoxels + 1 entries)
+// into the data and `times` arrays for unstructured data.  numItems: the
+// element count of each attribute array (validated as the reference does).
+OrcVolume *orc_dense_create_temporal(const int32_t dims[3], uint32_t numAttributes, const void *const *data,
+                                     const uint32_t *types, const uint64_t *numItems, int cellCentered,
+                                     const float gridOrigin[3], const float gridSpacing[3],
+                                     const float *indexToObject, const float *background, int numTimesteps,
+                                     const void *indices, uint32_t indexType, uint64_t numIndices,
+                                     const float *times, uint64_t numTimes);
+// Samples / gradients at per-point times (NULL: time 0) on `threads` host
+// threads.
+void orc_sample_times(const OrcVolume *v, int filter, uint64_t n, const float *points, const float *times,
+                      uint32_t attr, float *out, int threads);
+void orc_gradient_times(const OrcVolume *v, int filter, uint64_t n, const float *points, const float *times,
+                        uint32_t attr, float *out, int threads);
+// The density path tracer, one progressive frame added into rgba / weights
+// (pt: shutter, sigmaTScale, sigmaSScale, ambientLightIntensity, time; ipt:
+// motionBlur, maxNumScatters, showBbox, frame).
+void orc_path_trace(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint32_t attr,
+                    const float camera[14], const float *tfColors, int tfNum, const float tfRange[2], int W, int H,
+                    const float bounds[6], const float pt[5], const int ipt[4], float *rgba, float *weights);
 // orc_gradient split over `threads` host threads.
 void orc_gradient_parallel(const OrcVolume *v, int filter, uint32_t maxSamplingDepth, uint64_t n,
                            const float *points, uint32_t attr, float *out, int threads);

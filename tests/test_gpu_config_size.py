@@ -233,8 +233,12 @@ def test_vdb_4096_hits(vkl, vdb4096):
     k = np.minimum(gcnt, 16)
     mask = np.arange(16)[None, :] < k[:, None]
     np.testing.assert_array_equal(bits(got[mask]), bits(want[mask]))
+    # Against the FP-contraction build the hit counts are not exact: a march
+    # sample within rounding of an isovalue can change sides and add or drop
+    # a pair of hits (measured: 6 of these 65,536 rays, by 2).  The bound
+    # stated here is 0.05 % of the rays.
     fw, fcnt = vdb4096["fma"].hits(o, d, t, np.array([0.25, 0.5], np.float32), max_hits=16)
-    np.testing.assert_array_equal(gcnt, fcnt)
+    assert np.count_nonzero(gcnt != fcnt) <= len(o) // 2000
 
 
 def test_batched_64_volume_slice(vkl, device, oracle):

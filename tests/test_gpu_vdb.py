@@ -257,7 +257,8 @@ def test_vdb_volume_buffers_parameter_set(vkl, device, oracle):
 
 def test_dense_temporal_parameters(vkl, device, oracle):
     """structuredRegular: temporallyStructuredNumTimesteps = 0 means constant
-    data (DenseVdbVolume.cpp:149-186) and is accepted; > 0 is rejected."""
+    data (DenseVdbVolume.cpp:149-186) and is accepted; > 0 makes the data
+    temporally structured, which needs that many values per voxel."""
     vox = sinusoid_field((20, 18, 16), seed=2)
     v = vkl.Volume(device, "structuredRegular")
     v.set_vec3i("dimensions", (20, 18, 16))
@@ -268,7 +269,7 @@ def test_dense_temporal_parameters(vkl, device, oracle):
     pts = uniform_points(4000, (0, 0, 0), (19, 17, 15), seed=5)
     np.testing.assert_array_equal(bits(vkl.Sampler(v).sample(pts)), bits(ref.sample(pts)))
     v.set_int("temporallyStructuredNumTimesteps", 2)
-    with pytest.raises(vkl.VKLError, match="temporally varying"):
+    with pytest.raises(vkl.VKLError, match="has 5760 elements, but expected 11520"):
         v.commit()
 
 
