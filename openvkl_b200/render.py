@@ -41,6 +41,12 @@ class TransferFunction(C.Structure):
     _fields_ = [("valueRange", C.c_float * 2), ("numValues", C.c_int), ("colorsAndOpacities", C.c_float * (4 * MAX_TF))]
 
 
+class PathTracerParams(C.Structure):
+    _fields_ = [("shutter", C.c_float), ("motionBlur", C.c_int), ("sigmaTScale", C.c_float),
+                ("sigmaSScale", C.c_float), ("maxNumScatters", C.c_int), ("ambientLightIntensity", C.c_float),
+                ("showBbox", C.c_int), ("frame", C.c_uint)]
+
+
 class Params(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("attributeIndex", C.c_uint), ("time", C.c_float),
                 ("featureFlags", C.c_uint64), ("bounds", C.c_float * 6), ("samplingRate", C.c_float), ("intervalColorScale", C.c_float),
@@ -59,6 +65,10 @@ def load_library(path: str = LIB_PATH):
         L.vklExampleRender.restype = C.c_int
         L.vklExampleRender.argtypes = [C.c_int, vkl.VKLObject, vkl.VKLObject, vkl.VKLObject, C.POINTER(Camera),
                                        C.POINTER(TransferFunction), C.POINTER(Params), C.c_void_p, C.c_void_p]
+        L.vklExamplePathTrace.restype = C.c_int
+        L.vklExamplePathTrace.argtypes = [vkl.VKLObject, C.POINTER(Camera), C.POINTER(TransferFunction),
+                                          C.POINTER(Params), C.POINTER(PathTracerParams), C.c_void_p, C.c_void_p,
+                                          C.c_void_p]
         L.vklExampleSamplePoints.restype = C.c_int
         L.vklExampleSamplePoints.argtypes = [vkl.VKLObject, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
@@ -133,6 +143,35 @@ def render(renderer, sampler, camera, width, height, tf=None, interval_context=N
     if rc != 0:
         raise RuntimeError(f"vklExampleRender failed: CUDA error {rc}")
     return out
+
+
+def path_trace(sampler, camera, width, height, frames=(0,), tf=None, rgba=None, weights=None, stream=None,
+               time=0.0, shutter=0.0, motion_blur=False, sigma_t_scale=1.0, sigma_s_scale=1.0, max_num_scatters=1,
+               ambient_light_intensity=1.0, show_bbox=False, attr=0):
+    """The density path tracer: each frame adds one path per pixel into
+    rgba ((H, W, 4) CUDA tensor) and 1 into weights ((H, W)); the image is
+    rgba / weights.  Returns (rgba, weights)."""
+    import torch
+    L = load_library()
+    if tf is None:
+        lo, hi = sampler.volume.value_range()
+        tf = transfer_function((lo, hi))
+    prm = params(width, height, sampler.volume.bounding_box(), attr=attr)
+    prm.time = float(time)
+    prm.featureFlags = sampler.feature_flags()
+    if rgba is None:
+        rgba = torch.zeros((height, width, 4), dtype=torch.float32, device="cuda")
+    if weights is None:
+        weights = torch.zeros((height, width), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    for f in frames:
+        pt = PathTracerParams(float(shutter), int(motion_blur), float(sigma_t_scale), float(sigma_s_scale),
+                              int(max_num_scatters), float(ambient_light_intensity), int(show_bbox), int(f))
+        rc = L.vklExamplePathTrace(sampler.h, C.byref(camera), C.byref(tf), C.byref(prm), C.byref(pt),
+                                   rgba.data_ptr(), weights.data_ptr(), st)
+        if rc != 0:
+            raise RuntimeError(f"vklExamplePathTrace failed: CUDA error {rc}")
+    return rgba, weights
 
 
 def sample_points(sampler, points, attr=0):

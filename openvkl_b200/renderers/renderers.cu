@@ -11,6 +11,9 @@
 //   camera                   Camera.ih (Camera_createRay)
 //   transfer function        RendererGpuKernel.h:64-93 (sampleTransferFunction)
 //   box clip                 RendererGpuKernel.h:142-155 (intersectBox)
+//   density path tracer      density_path_tracer/DensityPathTracerGpuKernel.cpp:
+//                            9-170 (Woodcock tracking, isotropic scattering,
+//                            progressive accumulation), Random.ih (RandomTEA)
 //
 // One ray per pixel, through the pixel centre.  The reference's approximate
 // reciprocals and rsqrt (ISPC rcp / rsqrt, sycl::native::recip) are written
@@ -20,6 +23,7 @@
 #include <cstdint>
 
 #include "../../include/openvkl_cuda_device.h"
+#include "pt_math.h"
 
 extern "C" {
 
@@ -49,6 +53,18 @@ typedef struct {
   float intervalColorScale, intervalOpacity;  // interval iterator debug
   int firstIntervalOnly, showIntervalBorders;
 } VKLExampleParams;
+
+// Density path tracer parameters (DensityPathTracerParams.h) and the frame
+// index that seeds each pixel's random sequence.
+typedef struct {
+  float shutter;
+  int motionBlur;
+  float sigmaTScale, sigmaSScale;
+  int maxNumScatters;
+  float ambientLightIntensity;
+  int showBbox;
+  unsigned int frame;
+} VKLExamplePathTracerParams;
 
 }  // extern "C"
 
@@ -267,6 +283,137 @@ __global__ void __launch_bounds__(kThreads) kHitRenderer(VKLSampler sampler, VKL
   out[idx] = make_float4(color.x, color.y, color.z, 1.f);
 }
 
+// RandomTEA (Random.ih): 8 rounds of the tiny encryption algorithm per draw
+// of two floats in [0, 1).
+struct Tea {
+  uint32_t v0, v1;
+};
+__device__ __forceinline__ void teaFloats(Tea &r, float &a, float &b)
+{
+  uint32_t v0 = r.v0, v1 = r.v1, sum = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    sum += 0x9e3779b9u;
+    v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + sum) ^ ((v1 >> 5) + 0xc8013ea4u);
+    v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + sum) ^ ((v0 >> 5) + 0x7e95761eu);
+  }
+  r.v0 = v0;
+  r.v1 = v1;
+  const float tofloat = 2.3283064365386962890625e-10f;  // 2^-32
+  a                   = (float)v0 * tofloat;
+  b                   = (float)v1 * tofloat;
+}
+
+// Woodcock steps one tracking call may take: the tracking ends long before
+// on any volume (each step moves on by an exponential distance), the bound
+// only keeps a degenerate transfer function from looping.
+constexpr int kMaxWoodcockSteps = 1 << 16;
+
+// sampleWoodcock (DensityPathTracerGpuKernel.cpp:25-75): distance tracking
+// against the majorant sigmaTScale; true with the sample at the event.
+__device__ __forceinline__ bool sampleWoodcock(VKLSampler sampler, const VKLExampleTransferFunction &tf,
+                                               const VKLExampleParams &prm, const VKLExamplePathTracerParams &pt,
+                                               Tea &rng, v3 org, v3 dir, vkl_range1f hits, float &t, float &sample,
+                                               float &transmittance)
+{
+  t                    = hits.lower;
+  const float sigmaMax = pt.sigmaTScale;
+  if (sigmaMax <= 0.f) {
+    transmittance = 1.f;
+    return false;
+  }
+  for (int step = 0; step < kMaxWoodcockSteps; ++step) {
+    float r0, r1, s0, s1;
+    teaFloats(rng, r0, r1);
+    teaFloats(rng, s0, s1);
+    t = t + (-pt_log(1.f - r0)) / sigmaMax;
+    if (t > hits.upper) {
+      transmittance = 1.f;
+      return false;
+    }
+    const v3 c  = org + t * dir;
+    float time  = prm.time;
+    if (pt.motionBlur)
+      time = time + (s0 - 0.5f) * pt.shutter;
+    time = fminf(fmaxf(time, 0.f), 1.f);
+    const vkl_vec3f cv{c.x, c.y, c.z};
+    sample                   = vklComputeSample(&sampler, &cv, prm.attributeIndex, time, prm.featureFlags);
+    const v4 sc              = transfer(tf, sample);
+    const float sigmaTSample = sigmaMax * sc.w;
+    if (r1 < sigmaTSample / sigmaMax)
+      break;
+  }
+  transmittance = 0.f;
+  return true;
+}
+
+// integrate + renderPixel (DensityPathTracerGpuKernel.cpp:77-163): scatter
+// until the path leaves the volume or maxNumScatters, ambient light picked
+// up by secondary paths, accumulated into rgba / weight.
+__global__ void __launch_bounds__(kThreads) kDensityPathTracer(VKLSampler sampler,
+                                                               const __grid_constant__ VKLExampleCamera cam,
+                                                               const __grid_constant__ VKLExampleTransferFunction tf,
+                                                               const __grid_constant__ VKLExampleParams prm,
+                                                               const __grid_constant__ VKLExamplePathTracerParams pt,
+                                                               float4 *rgba, float *weight)
+{
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= prm.width * prm.height)
+    return;
+  v3 org, dir;
+  pixelRay(cam, prm, idx, org, dir);
+  Tea rng{pt.frame, (uint32_t)idx};
+  int maxScatterIndex      = 0;
+  bool primaryRayIntersect = false;
+  v3 Le = {0.f, 0.f, 0.f}, sigmaS = {0.f, 0.f, 0.f};
+  for (int scatterIndex = 0; true; scatterIndex++) {
+    float sample    = 0.f;
+    maxScatterIndex = max(scatterIndex, maxScatterIndex);
+    const vkl_range1f rt = intersectBox(org, dir, prm.bounds);
+    const bool empty     = rt.lower > rt.upper;
+    if (scatterIndex == 0 && !empty)
+      primaryRayIntersect = true;
+    if (empty)
+      break;
+    float t = 0.f, transmittance = 0.f;
+    if (!sampleWoodcock(sampler, tf, prm, pt, rng, org, dir, rt, t, sample, transmittance)) {
+      if (scatterIndex > 0) {
+        const float a = transmittance * pt.ambientLightIntensity;
+        Le            = Le + v3{a * sigmaS.x, a * sigmaS.y, a * sigmaS.z};
+      }
+      break;
+    }
+    if (scatterIndex >= pt.maxNumScatters)
+      break;
+    const v4 sc = transfer(tf, sample);
+    sigmaS      = {pt.sigmaSScale * sc.x * sc.w, pt.sigmaSScale * sc.y * sc.w, pt.sigmaSScale * sc.z * sc.w};
+    org         = org + t * dir;
+    // uniformSampleSphere(1, s) (Random.ih:57-63)
+    float s0, s1;
+    teaFloats(rng, s0, s1);
+    const float phi      = 6.28318530717958647692f * s0;
+    const float cosTheta = 1.f * (1.f - 2.f * s1);
+    const float sinTheta = 2.f * 1.f * sqrtf(s1 * (1.f - s1));
+    float sinPhi, cosPhi;
+    pt_sincos(phi, &sinPhi, &cosPhi);
+    dir = {cosPhi * sinTheta, sinPhi * sinTheta, cosTheta};
+  }
+  v3 color    = Le;
+  float alpha = maxScatterIndex > 0 ? 1.f : 0.f;
+  if (pt.showBbox && primaryRayIntersect) {
+    const float blend = 0.2f;
+    alpha             = (1.f - blend) * alpha + blend * 1.f;
+    color             = (1.f - blend) * color + v3{blend * 1.f, blend * 1.f, blend * 1.f};
+  }
+  float4 acc  = rgba[idx];
+  acc.x       = acc.x + color.x;
+  acc.y       = acc.y + color.y;
+  acc.z       = acc.z + color.z;
+  acc.w       = acc.w + alpha;
+  rgba[idx]   = acc;
+  weight[idx] = weight[idx] + 1.f;
+}
+
 // User code sampling its own points with the device API: sample and
 // gradient of every point (the per-point analogue of vklComputeSampleN /
 // vklComputeGradientN).
@@ -314,6 +461,22 @@ __attribute__((visibility("default"))) int vklExampleRender(int renderer, VKLSam
     kHitRenderer<<<blocks, kThreads, 0, st>>>(sampler, hitContext, *camera, *tf, *params, (float4 *)rgba);
   else
     return (int)cudaErrorInvalidValue;
+  return (int)cudaGetLastError();
+}
+
+// One progressive frame of the density path tracer: adds each pixel's
+// radiance and alpha to rgba (width*height float4) and 1 to its weight.
+__attribute__((visibility("default"))) int vklExamplePathTrace(VKLSampler sampler, const VKLExampleCamera *camera,
+                                                               const VKLExampleTransferFunction *tf,
+                                                               const VKLExampleParams *params,
+                                                               const VKLExamplePathTracerParams *pt, float *rgba,
+                                                               float *weights, void *stream)
+{
+  const int n = params->width * params->height;
+  if (n <= 0)
+    return 0;
+  kDensityPathTracer<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      sampler, *camera, *tf, *params, *pt, (float4 *)rgba, weights);
   return (int)cudaGetLastError();
 }
 
