@@ -29,7 +29,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,
 
 SOURCES = ["api.cpp", "objects.cpp", "k_sample.cu", "k_sample_nearest.cu", "k_sample_linear.cu",
            "k_sample_cubic.cu", "k_build.cu", "k_iterate.cu", "k_noalloc.cu", "k_batch.cu", "k_surrogate.cu",
-           "k_bin.cu", "k_macrocell.cu", "k_temporal.cu"]
+           "k_bin.cu", "k_macrocell.cu", "k_temporal.cu", "k_sample_rays.cu"]
 
 
 # The example renderers (a consumer of the __device__ API, built separately

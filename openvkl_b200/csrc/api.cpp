@@ -248,6 +248,33 @@ void sampleTemporal(Device *d, Sampler *s, uint64_t N, const void *pts, const fl
 // `times`: one time per point (host or device memory), or NULL for time 0;
 // only temporally varying volumes read them (the reference's temporally
 // constant volumes ignore the time as well).
+// Ray-run sampling (k_sample_rays.cu) of large dense float trilinear calls
+// whose points come as runs of samples per ray; the run length is detected
+// once per call (on its first chunk).  Returns false where the ordinary
+// launch is to run.
+bool rayRuns(Device *d, Sampler *s, int filter, uint64_t n, const float *pts, uint32_t attr, float *out, bool grad,
+             int &runS)
+{
+  const DevGrid &g = s->volume->grid;
+  if (!d->rayRuns || !rayRunsApply(g, filter, attr) || n < (1u << 20) || s->s.maxSamplingDepth < kNumLevels - 1)
+    return false;
+  std::lock_guard<std::mutex> lock(d->runMutex);
+  if (runS < 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaCheck(cudaStreamIsCapturing(d->stream, &cs), "capture status");
+    // the detector reads back its counters: not while the stream is captured
+    runS = cs == cudaStreamCaptureStatusNone ? detectRayRuns(g, n, pts, d->runScratch, d->stream) : 0;
+    if (runS > 0)
+      d->log(VKL_LOG_DEBUG, "sampling " + std::to_string(n) + " points as runs of " + std::to_string(runS) +
+                                " samples per ray\n");
+  }
+  if (runS <= 0)
+    return false;
+  launchSampleRays(s->launchGrid(), s->s.maxSamplingDepth, n, pts, attr, out, grad, runS, d->runScratch,
+                   d->stream);
+  return true;
+}
+
 void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float *out,
              uint32_t M, const uint32_t *attrs, const float *times = nullptr)
 {
@@ -266,8 +293,11 @@ void sampleN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, float 
     sampleTemporal(d, s, N, pts, times, out, M, attrs, false);
     return;
   }
+  int runS = -1;
   staged(d, N, 12, pts, 4 * M, out, [&](uint64_t n, const void *din, void *dout) {
     if (M == 1 && binned(d, s, s->s.filter, n, (const float *)din, attrs[0], (float *)dout, false))
+      return;
+    if (M == 1 && rayRuns(d, s, s->s.filter, n, (const float *)din, attrs[0], (float *)dout, false, runS))
       return;
     launchSample(s->launchGrid(), s->s.filter, s->s.maxSamplingDepth, n, (const float *)din, M,
                  attrs, (float *)dout, d->stream);
@@ -289,8 +319,11 @@ void gradientN(const VKLSampler *sampler, uint64_t N, const vkl_vec3f *pts, vkl_
     sampleTemporal(d, s, N, pts, times, out, 1, &attr, true);
     return;
   }
+  int runS = -1;
   staged(d, N, 12, pts, 12, out, [&](uint64_t n, const void *din, void *dout) {
     if (binned(d, s, s->s.gradientFilter, n, (const float *)din, attr, (float *)dout, true))
+      return;
+    if (rayRuns(d, s, s->s.gradientFilter, n, (const float *)din, attr, (float *)dout, true, runS))
       return;
     launchGradient(s->launchGrid(), s->s.gradientFilter, s->s.maxSamplingDepth, n,
                    (const float *)din, attr, (float *)dout, d->stream);
@@ -486,6 +519,8 @@ void vklDeviceSetInt(VKLDevice dev, const char *name, int x)
     d->binning = x != 0;
   if (!std::strcmp(name, "textureSampling"))
     d->textureSampling = x != 0;
+  if (!std::strcmp(name, "rayRunSampling"))
+    d->rayRuns = x != 0;
 }
 
 void vklDeviceSetString(VKLDevice dev, const char *name, const char *s)

@@ -162,6 +162,21 @@ struct DeviceBuffer {
 // ---------------------------------------------------------------------------
 // Device.
 // ---------------------------------------------------------------------------
+// Device scratch of the ray-run sampling path (k_sample_rays.cu): the
+// detector's counters and the kernels' error word.
+struct RunScratch {
+  DeviceBuffer counts;
+};
+// Ray-run sampling of dense float volumes with the trilinear filter:
+// rayRunsApply says whether the path covers the call, detectRayRuns returns
+// the run length S the points are laid out in (0: not ray runs; reads back
+// a few counters, so it synchronizes the stream), launchSampleRays samples
+// (grad: gradients) as launchSample / launchGradient do.
+bool rayRunsApply(const DevGrid &g, int filter, uint32_t attr);
+int detectRayRuns(const DevGrid &g, uint64_t n, const float *pts, RunScratch &scratch, cudaStream_t stream);
+void launchSampleRays(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float *pts, uint32_t attr, float *out,
+                      bool grad, int S, RunScratch &scratch, cudaStream_t stream);
+
 // Device scratch of binned sampling (launchSampleBinned): detection
 // counters, the binned entries of one pass, bin histogram and cursors.
 struct BinScratch {
@@ -219,6 +234,11 @@ struct Device {
   // "binnedSampling" 0 turns it off.
   std::mutex binMutex;
   BinScratch binScratch;
+  // ray-run detection and kernel scratch; `runMutex` serialises its users;
+  // device parameter "rayRunSampling" 0 turns the path off
+  std::mutex runMutex;
+  RunScratch runScratch;
+  bool rayRuns = true;
   bool binning = true;
   // Texture atlases of dense float attributes (DevGrid::atlasTex): on by
   // default; device parameter "textureSampling" 0 turns them off for volumes

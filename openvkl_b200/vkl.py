@@ -125,6 +125,7 @@ class vvec3f16(C.Structure):
 
 
 _ERROR_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_char_p)
+_LOG_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_char_p)
 _lib = None
 
 
@@ -142,6 +143,7 @@ def load_library(path: str = LIB_PATH, load_only: bool = False) -> C.CDLL:
         "vklInit": (None, []),
         "vklNewDevice": (P, [C.c_char_p]),
         "vklDeviceSetErrorCallback": (None, [P, _ERROR_CB, VP]),
+        "vklDeviceSetLogCallback": (None, [P, _LOG_CB, VP]),
         "vklDeviceSetInt": (None, [P, C.c_char_p, I]),
         "vklDeviceSetString": (None, [P, C.c_char_p, C.c_char_p]),
         "vklDeviceSetVoidPtr": (None, [P, C.c_char_p, VP]),
@@ -296,6 +298,12 @@ class Device:
 
     def set_int(self, name: str, value: int):
         self.lib.vklDeviceSetInt(self.handle, name.encode(), int(value))
+
+    def capture_log(self, messages: list):
+        """Routes the device's log messages into `messages` (a list of str);
+        vklDeviceSetLogCallback."""
+        self._log_cb = _LOG_CB(lambda user, msg: messages.append(msg.decode() if msg else ""))
+        self.lib.vklDeviceSetLogCallback(self.handle, self._log_cb, None)
 
     def set_stream(self, stream_ptr: int):
         self.lib.vklDeviceSetVoidPtr(self.handle, b"cudaStream", C.c_void_p(stream_ptr))
