@@ -12,9 +12,9 @@
 // order is read off the layout, and shared memory only stages the runs:
 //  - the 8 runs are copied into padded shared-memory rows by 8 bulk copies
 //    (cp.async.bulk, completion on an mbarrier, bounded wait);
-//  - the results are staged in padded rows and written back by 8 bulk copies;
-//  - the row pitches (3 S + 4 and S + 4 words) make every lane's loads and
-//    stores fall in distinct banks.
+//  - the row pitch (3 S + 4 words) puts every lane's loads in distinct
+//    banks;
+//  - the results go straight to global memory.
 // Each point is computed by the same code as in the other kernels, so the
 // results do not depend on the order.  A detector (kDetectRuns) picks S from
 // the points themselves: it counts, on a sample of warps, the distinct
@@ -52,11 +52,10 @@ __device__ __forceinline__ bool waitPhase0(uint64_t *bar)
   return false;
 }
 
-template <int S, int OUTF>
+template <int S>
 struct RunSmem {
-  static constexpr int kPtPitch  = 3 * S + 4;     // words
-  static constexpr int kOutPitch = OUTF * S + 4;  // words
-  static constexpr size_t bytes  = 16 + 4 * (size_t)kRuns * (kPtPitch + kOutPitch);
+  static constexpr int kPtPitch = 3 * S + 4;  // words
+  static constexpr size_t bytes = 16 + 4 * (size_t)kRuns * kPtPitch;
 };
 
 // At least 5 CTAs per SM (51 registers) for the texture-atlas field, whose
@@ -72,17 +71,15 @@ __global__ void __launch_bounds__(kRunThreads, runMinBlocks<Field>())
     kSampleRuns(const __grid_constant__ DevGrid g, uint32_t maxDepth, uint64_t n, const float *__restrict__ pts,
                 uint32_t attr, float *__restrict__ out, uint32_t *__restrict__ error)
 {
-  constexpr int OUTF = GRAD ? 3 : 1;
-  using L            = RunSmem<S, OUTF>;
+  using L            = RunSmem<S>;
   constexpr int TILE = kRuns * S;
   constexpr int PPT  = TILE / kRunThreads;
   extern __shared__ __align__(128) unsigned char smemRaw[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smemRaw);
   float *rows   = reinterpret_cast<float *>(smemRaw + 16);
-  float *res    = rows + kRuns * L::kPtPitch;
   const uint64_t base = (uint64_t)blockIdx.x * TILE;
-  // whole tiles of 16-byte aligned arrays go through the bulk copies
-  const bool bulk = base + TILE <= n && ((reinterpret_cast<uintptr_t>(pts) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+  // whole tiles of 16-byte aligned point arrays go through the bulk copies
+  const bool bulk = base + TILE <= n && (reinterpret_cast<uintptr_t>(pts) & 15) == 0;
   if (bulk && threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -111,70 +108,31 @@ __global__ void __launch_bounds__(kRunThreads, runMinBlocks<Field>())
   }
   const bool cc = g.constantCellData != 0;
   const Field F = makeField<Field>(g, attr, maxDepth);
-  // Groups of G points: their coordinates are read into registers, then all
-  // G are sampled, then the results stored.  The point rows and the result
-  // rows share one shared-memory array, so a result store between two
-  // samples would keep the compiler from overlapping their gathers.
-  constexpr int G = PPT < 4 ? PPT : 4;
-  static_assert(PPT % G == 0, "group size");
-#pragma unroll 1
-  for (int j0 = 0; j0 < PPT; j0 += G) {
-    f3 p[G];
-    float v[G][OUTF];
+  // Results go straight to global memory: a warp's stores are 8 runs x 4
+  // consecutive samples, 8 segments of 16 B (48 B for gradients).  Staging
+  // them in shared memory between the samples (the rows share one array)
+  // kept the compiler from overlapping consecutive samples' gathers: 7.85 vs
+  // 3.57 ms on the 1024^3 coherent workload.
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
-      const int k    = threadIdx.x + (j0 + j) * kRunThreads;
-      const float *q = rows + (k & (kRuns - 1)) * L::kPtPitch + 3 * (k >> 3);
-      p[j]           = xfmPoint(g.objectToIndex, f3{q[0], q[1], q[2]});
-    }
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
+  for (int j = 0; j < PPT; ++j) {
+    const int k      = threadIdx.x + j * kRunThreads;
+    const int r      = k & (kRuns - 1), s = k >> 3;
+    const uint64_t i = base + (uint64_t)r * S + s;
+    if (i < n) {
+      const float *q = rows + r * L::kPtPitch + 3 * s;
+      const f3 p     = xfmPoint(g.objectToIndex, f3{q[0], q[1], q[2]});
       if constexpr (GRAD) {
         f3 gr = {0.f, 0.f, 0.f};
         if constexpr (FILTER == kFilterCubic)
-          gr = xfmNormal(g.objectToIndex, gradientCubic(F, p[j]));
+          gr = xfmNormal(g.objectToIndex, gradientCubic(F, p));
         else if constexpr (FILTER == kFilterLinear)
-          gr = xfmNormal(g.objectToIndex, gradientLinear(F, p[j]));
-        v[j][0]                = gr.x;
-        v[j][OUTF > 1 ? 1 : 0] = gr.y;
-        v[j][OUTF > 2 ? 2 : 0] = gr.z;
+          gr = xfmNormal(g.objectToIndex, gradientLinear(F, p));
+        __stcs(out + 3 * i, gr.x);
+        __stcs(out + 3 * i + 1, gr.y);
+        __stcs(out + 3 * i + 2, gr.z);
       } else {
-        v[j][0] = filterAt<Field, FILTER>(F, cc, p[j]);
+        __stcs(out + i, filterAt<Field, FILTER>(F, cc, p));
       }
-    }
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
-      const int k = threadIdx.x + (j0 + j) * kRunThreads;
-      const int r = k & (kRuns - 1), s = k >> 3;
-      if (base + (uint64_t)r * S + s < n) {
-        float *o = res + r * L::kOutPitch + OUTF * s;
-#pragma unroll
-        for (int c = 0; c < OUTF; ++c)
-          o[c] = v[j][c];
-      }
-    }
-  }
-  if (bulk) {
-    // generic-proxy writes of res, then the bulk copies read them
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll 1
-      for (int r = 0; r < kRuns; ++r)
-        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
-                         out + OUTF * (base + (uint64_t)r * S)),
-                     "r"(smemAddr(res + r * L::kOutPitch)), "r"(S * OUTF * 4)
-                     : "memory");
-      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-    }
-  } else {
-    __syncthreads();
-    for (int k = threadIdx.x; k < TILE * OUTF; k += kRunThreads) {
-      const int r = k / (OUTF * S), w = k - r * OUTF * S;
-      const uint64_t e = OUTF * base + (uint64_t)k;
-      if (e < OUTF * n)
-        out[e] = res[r * L::kOutPitch + w];
     }
   }
 }
@@ -215,7 +173,7 @@ template <class Field, int FILTER, bool GRAD, int S>
 void launchRuns(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float *pts, uint32_t attr, float *out,
                 uint32_t *error, cudaStream_t st)
 {
-  constexpr size_t smem = RunSmem<S, GRAD ? 3 : 1>::bytes;
+  constexpr size_t smem = RunSmem<S>::bytes;
   // the dynamic shared-memory limit is raised once per instantiation and
   // device (bit = device ordinal)
   static std::atomic<uint64_t> configured{0};
