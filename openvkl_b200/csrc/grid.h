@@ -24,17 +24,17 @@ constexpr uint32_t kMaxAttributes = 16;
 constexpr uint32_t kLeafRes    = 8;
 constexpr uint32_t kLeafVoxels = 512;
 
-VKL_HD uint32_t logRes(uint32_t l)
+constexpr VKL_HD uint32_t logRes(uint32_t l)
 {
   return l == 0 ? 6u : l == 1 ? 5u : l == 2 ? 4u : l == 3 ? 3u : 0u;
 }
-VKL_HD uint32_t totalLogRes(uint32_t l)
+constexpr VKL_HD uint32_t totalLogRes(uint32_t l)
 {
   return l == 0 ? 18u : l == 1 ? 12u : l == 2 ? 7u : l == 3 ? 3u : 0u;
 }
 // Resolution of a level-l node in leaf voxels; level 4 (one past the leaf)
 // is 1, the DDA's elementary cell.
-VKL_HD uint32_t levelRes(uint32_t l) { return 1u << totalLogRes(l); }
+constexpr VKL_HD uint32_t levelRes(uint32_t l) { return 1u << totalLogRes(l); }
 VKL_HD uint64_t levelNumVoxels(uint32_t l) { return 1ull << (3 * logRes(l)); }
 
 // Data type codes (VKLDataType values of the public API).
@@ -153,7 +153,7 @@ struct DevGrid {
   // 2x2x2 corners from it with two tld4 footprint gathers; z-neighbours sit
   // side by side in the atlas, a few KB apart.
   uint64_t atlasTex[kMaxAttributes];
-  uint32_t atlasPlanesPerRow;
+  uint32_t atlasPlanesPerRow;  // a power of two
   // Temporally varying (motion-blur) dense data, kept as given (x fastest,
   // each voxel's time samples consecutive, not bricked): 0 = constant,
   // 1 = structured (numTimesteps values per voxel, regularly placed in

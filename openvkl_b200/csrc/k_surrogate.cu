@@ -24,6 +24,7 @@
 // the FP32 master parameters and refreshes their FP16 copies.
 #include <cuda_fp16.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -32,6 +33,7 @@
 #include "kernels.h"
 #include "objects.h"
 #include "sampling.cuh"
+#include "tcgen05.cuh"
 
 namespace vklcuda {
 
@@ -286,48 +288,170 @@ __device__ __forceinline__ void forwardChunk(const FwdWeights &W, const __half *
 // ---------------------------------------------------------------------------
 // Inference (optionally with the plain fallback) and calibration.
 // MODE 0: samples; MODE 1: calibration (region error of the network).
+//
+// A CTA of 256 threads runs two independent groups of 128 (own named
+// barrier, mbarrier and TMEM columns); a group owns a 128-point tile:
+// thread r encodes point r into row r of the group's operand buffer in
+// shared memory; each hidden layer is then one 128 x 64 tensor-core product
+// (tcgen05.mma, M = 128, N = 64, K = 32 or 64, FP16 operands, FP32
+// accumulator in tensor memory) issued by the group's first thread, and
+// thread r reads its row back from TMEM lane r (tcgen05.ld), applies ReLU,
+// rounds to FP16 and writes the next layer's operand row into the same
+// buffer (the product that read it has completed).  The 64 -> 1 output layer
+// is a dot product on the CUDA cores.  The weights stay in shared memory for
+// the CTA's lifetime (persistent over tiles).
 // ---------------------------------------------------------------------------
-template <class Field, int MODE>
-__global__ void __launch_bounds__(kThr) kSurrogateInfer(const __grid_constant__ Encoding E,
-                                                        const __half2 *__restrict__ table,
-                                                        const __half *__restrict__ w16,
-                                                        const __grid_constant__ DevGrid g,
-                                                        const __grid_constant__ Judge J, uint64_t n,
-                                                        const float *__restrict__ pts, float *__restrict__ out,
-                                                        int fallback)
+constexpr int kInferThr   = 256;  // two groups of 128 threads
+constexpr int kInferCtasPerSM = 3;
+constexpr uint32_t kTcCols = 128;  // TMEM columns per CTA: one 64-column accumulator per group
+
+struct TcInferSmem {                // operand buffers on 1024-byte boundaries
+  unsigned char act[2][kTile * 128];  // per group: layer-1 operand (K = 32 of 64), then hidden activations
+  unsigned char w1[kH * 128];         // K = 32 of 64 used
+  unsigned char w2[kH * 128];
+  unsigned char w3[kH * 128];
+  float w4[kH];
+  uint64_t bar[2];
+  uint32_t tmem;
+};
+constexpr size_t kTcInferSmemBytes = sizeof(TcInferSmem) + 1024;  // + alignment slack
+
+// Rows of a row-major [rows][k] FP16 matrix into the swizzled K-major layout.
+__device__ __forceinline__ void loadSwizzledRows(unsigned char *dst, const __half *__restrict__ src, int rows, int k)
 {
-  __shared__ FwdWeights W;
-  __shared__ __align__(16) __half X[kTile][kIn + 8];
-  __shared__ float ys[kTile];
-  loadFwdWeights(W, w16);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
-  for (uint64_t base = (uint64_t)blockIdx.x * kTile; base < n; base += (uint64_t)gridDim.x * kTile) {
-    const uint64_t i = base + threadIdx.x;
+  const int cpr = k / 8;
+  for (int idx = threadIdx.x; idx < rows * cpr; idx += blockDim.x) {
+    const int r = idx / cpr, c = idx - r * cpr;
+    *reinterpret_cast<uint4 *>(dst + tc::swizzledChunk(r, c)) =
+        __ldg(reinterpret_cast<const uint4 *>(src + (size_t)r * k) + c);
+  }
+}
+
+__device__ __forceinline__ uint32_t reluPack(uint32_t lo, uint32_t hi)
+{
+  return pack(fmaxf(__uint_as_float(lo), 0.f), fmaxf(__uint_as_float(hi), 0.f));
+}
+
+// Barrier of one 128-thread group; returns whether any thread passed true.
+__device__ __forceinline__ bool groupSyncOr(uint32_t id, bool v)
+{
+  uint32_t r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 q, %1, 0; bar.red.or.pred p, %2, 128, q; selp.u32 %0, 1, 0, p; }"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+template <class Field, int MODE>
+__global__ void __launch_bounds__(kInferThr, kInferCtasPerSM)
+    kSurrogateInfer(const __grid_constant__ Encoding E, const __half2 *__restrict__ table,
+                    const __half *__restrict__ w16, const __grid_constant__ DevGrid g,
+                    const __grid_constant__ Judge J, uint64_t n, const float *__restrict__ pts,
+                    float *__restrict__ out, int fallback, uint32_t *__restrict__ err)
+{
+  extern __shared__ unsigned char smemRaw[];
+  TcInferSmem &S = *reinterpret_cast<TcInferSmem *>(smemRaw + ((1024u - (tc::smemAddr(smemRaw) & 1023u)) & 1023u));
+  const int warp = threadIdx.x >> 5;
+  const int grp  = threadIdx.x >> 7;
+  const uint32_t row = threadIdx.x & 127u;
+  loadSwizzledRows(S.w1, w16 + kOffW1, kH, kIn);
+  loadSwizzledRows(S.w2, w16 + kOffW2, kH, kH);
+  loadSwizzledRows(S.w3, w16 + kOffW3, kH, kH);
+  for (int k = threadIdx.x; k < kH; k += kInferThr)
+    S.w4[k] = __half2float(w16[kOffW4 + k]);
+  if (threadIdx.x == 0) {
+    tc::mbarInit(&S.bar[0], 1);
+    tc::mbarInit(&S.bar[1], 1);
+  }
+  if (warp == 0)
+    tc::tmemAlloc(&S.tmem, kTcCols);
+  tc::fenceProxyAsync();
+  tc::fenceBeforeSync();
+  __syncthreads();
+  tc::fenceAfterSync();
+  // this group's accumulator: columns 64 grp..; this warp's lanes 32 (warp % 4)..
+  const uint32_t acc   = S.tmem + 64u * grp;
+  const uint32_t myRow = acc + ((uint32_t)(32 * (warp & 3)) << 16);
+  constexpr uint32_t idesc = tc::f16InstrDesc(kTile, kH);
+  unsigned char *buf   = S.act[grp];
+  const uint32_t bufA  = tc::smemAddr(buf);
+  uint64_t *bar        = &S.bar[grp];
+  const uint32_t barId = 1u + grp;
+  uint32_t phase = 0;
+  bool ok        = true;
+  for (uint64_t base = ((uint64_t)blockIdx.x * 2 + grp) * kTile; base < n && ok;
+       base += (uint64_t)gridDim.x * 2 * kTile) {
+    const uint64_t i = base + row;
     f3 p             = {0.f, 0.f, 0.f};
-    __half2 *row     = reinterpret_cast<__half2 *>(&X[threadIdx.x][0]);
+    __half2 feat[kLv];
     if (i < n) {
       p = {__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2)};
       float u[3];
       unitPosition(E, p, u);
-      encodePoint<kLv>(E, table, u, row);
+      encodePoint<kLv>(E, table, u, feat);
     } else {
-      for (int k = 0; k < kLv; ++k)
-        row[k] = __floats2half2_rn(0.f, 0.f);
-    }
-    __syncthreads();
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const int m0 = 32 * warp + 16 * c;
-      float y0, y1;
-      forwardChunk(W, &X[0][0], kIn + 8, m0, gq, tq, y0, y1, nullptr, 0);
-      if (tq == 0) {
-        ys[m0 + gq]     = y0;
-        ys[m0 + gq + 8] = y1;
+      for (int k = 0; k < kLv; ++k)
+        feat[k] = __floats2half2_rn(0.f, 0.f);
+    }
+#pragma unroll
+    for (int c = 0; c < kIn / 8; ++c) {
+      uint4 v;
+      v.x = *reinterpret_cast<const uint32_t *>(&feat[4 * c]);
+      v.y = *reinterpret_cast<const uint32_t *>(&feat[4 * c + 1]);
+      v.z = *reinterpret_cast<const uint32_t *>(&feat[4 * c + 2]);
+      v.w = *reinterpret_cast<const uint32_t *>(&feat[4 * c + 3]);
+      *reinterpret_cast<uint4 *>(buf + tc::swizzledChunk(row, c)) = v;
+    }
+    float y = 0.f;
+#pragma unroll 1
+    for (int layer = 0; layer < 3; ++layer) {
+      // every thread's operand row is written -> one thread issues the layer
+      tc::fenceProxyAsync();
+      tc::fenceBeforeSync();
+      groupSyncOr(barId, false);
+      if (row == 0) {
+        tc::fenceAfterSync();
+        const uint32_t w = tc::smemAddr(layer == 0 ? S.w1 : layer == 1 ? S.w2 : S.w3);
+        const int ks     = layer == 0 ? kIn / 16 : kH / 16;
+        for (int k = 0; k < ks; ++k)
+          tc::mmaF16(acc, tc::sw128Desc(bufA + 32u * k), tc::sw128Desc(w + 32u * k), idesc, k > 0);
+        tc::commitTo(bar);
+      }
+      const bool done = tc::mbarWait(bar, phase);
+      phase ^= 1u;
+      if (groupSyncOr(barId, !done)) {
+        ok = false;
+        break;
+      }
+      tc::fenceAfterSync();
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[32];
+        tc::tmemLoad32(myRow + 32u * half, r);
+        tc::tmemLoadWait();
+        if (layer < 2) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint4 v;
+            v.x = reluPack(r[8 * q], r[8 * q + 1]);
+            v.y = reluPack(r[8 * q + 2], r[8 * q + 3]);
+            v.z = reluPack(r[8 * q + 4], r[8 * q + 5]);
+            v.w = reluPack(r[8 * q + 6], r[8 * q + 7]);
+            *reinterpret_cast<uint4 *>(buf + tc::swizzledChunk(row, 4 * half + q)) = v;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            y += __half2float(__float2half_rn(fmaxf(__uint_as_float(r[j]), 0.f))) * S.w4[32 * half + j];
+        }
       }
     }
-    __syncthreads();
+    if (!ok)
+      break;
     if (i < n) {
-      float y = ys[threadIdx.x];
       if (MODE == 0) {
         if (fallback) {
           const int64_t r = regionOf(g, J, p);
@@ -339,14 +463,19 @@ __global__ void __launch_bounds__(kThr) kSurrogateInfer(const __grid_constant__ 
         const int64_t r = regionOf(g, J, p);
         const float ref = plainSample<Field>(g, J, p);
         if (r >= 0 && !isnan(ref)) {
-          const float err = fabsf(y - ref);
-          atomicMax(reinterpret_cast<unsigned int *>(J.regionErr) + r, __float_as_uint(isnan(err) ? INFINITY : err));
+          const float e = fabsf(y - ref);
+          atomicMax(reinterpret_cast<unsigned int *>(J.regionErr) + r, __float_as_uint(isnan(e) ? INFINITY : e));
           J.regionSeen[r] = 1u;
         }
       }
     }
-    __syncthreads();
   }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (warp == 0)
+    tc::tmemDealloc(S.tmem, kTcCols);
+  if (!ok && row == 0)
+    atomicExch(err, 1u);
 }
 
 __global__ void kRegionFlags(uint64_t n, const float *regionErr, const uint32_t *seen, float threshold,
@@ -643,6 +772,8 @@ struct Surrogate {
   int step    = 0;
   int numSMs  = 0;
   bool dense  = false;
+  uint32_t *errHost = nullptr;  // host-mapped timeout flag of the inference kernel
+  uint32_t *errDev  = nullptr;
 
   void zeroGrads(cudaStream_t st)
   {
@@ -679,18 +810,48 @@ struct Surrogate {
     cudaCheck(cudaGetLastError(), "adam kernel");
   }
 
+  template <class Field, int MODE>
+  void inferWith(uint64_t n, const float *pts, float *out, int fallback, cudaStream_t st)
+  {
+    // the dynamic shared-memory limit is raised once per instantiation and
+    // device (bit = device ordinal)
+    static std::atomic<uint64_t> configured{0};
+    const uint64_t bit = 1ull << (device->cudaDevice & 63);
+    if (!(configured.load() & bit)) {
+      cudaCheck(cudaFuncSetAttribute(kSurrogateInfer<Field, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kTcInferSmemBytes),
+                "smem attribute");
+      configured.fetch_or(bit);
+    }
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, 2 * kTile), (uint64_t)numSMs * kInferCtasPerSM);
+    kSurrogateInfer<Field, MODE><<<grid, kInferThr, kTcInferSmemBytes, st>>>(
+        E, table16.as<__half2>(), w16.as<__half>(), sampler->volume->grid, J, n, pts, out, fallback, errDev);
+    cudaCheck(cudaGetLastError(), "surrogate kernel");
+  }
+
   template <int MODE>
   void infer(uint64_t n, const float *pts, float *out, int fallback, cudaStream_t st)
   {
-    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, kTile), (uint64_t)numSMs * 8);
-    const DevGrid &g    = sampler->volume->grid;
     if (dense)
-      kSurrogateInfer<DenseField<float>, MODE><<<grid, kThr, 0, st>>>(E, table16.as<__half2>(), w16.as<__half>(),
-                                                                     g, J, n, pts, out, fallback);
+      inferWith<DenseField<float>, MODE>(n, pts, out, fallback, st);
     else
-      kSurrogateInfer<SparseField<float>, MODE><<<grid, kThr, 0, st>>>(E, table16.as<__half2>(), w16.as<__half>(),
-                                                                      g, J, n, pts, out, fallback);
-    cudaCheck(cudaGetLastError(), "surrogate kernel");
+      inferWith<SparseField<float>, MODE>(n, pts, out, fallback, st);
+  }
+
+  // A tensor-core wait of an earlier inference launch that gave up sets a
+  // word of host-mapped memory; the next call reports it.
+  void checkTimeout()
+  {
+    if (errHost && *(volatile uint32_t *)errHost) {
+      *(volatile uint32_t *)errHost = 0u;
+      fail("surrogate: a tensor-core completion wait of an earlier inference launch timed out", VKL_UNKNOWN_ERROR);
+    }
+  }
+
+  ~Surrogate()
+  {
+    if (errHost)
+      cudaFreeHost(errHost);
   }
 };
 
@@ -787,6 +948,9 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLCudaSurrogate vklCudaNewSurrogate(VKLSample
     s->J.regionErr  = s->regionErr.as<float>();
     s->J.regionSeen = s->regionSeen.as<uint32_t>();
     cudaCheck(cudaDeviceGetAttribute(&s->numSMs, cudaDevAttrMultiProcessorCount, d->cudaDevice), "attribute");
+    cudaCheck(cudaHostAlloc((void **)&s->errHost, 4, cudaHostAllocMapped), "surrogate error flag");
+    *s->errHost = 0u;
+    cudaCheck(cudaHostGetDevicePointer((void **)&s->errDev, s->errHost, 0), "surrogate error flag");
     return (VKLCudaSurrogate)s;
   } catch (const VklError &e) {
     delete s;
@@ -886,6 +1050,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateCalibrate(VKLCudaSurr
   Surrogate *s = (Surrogate *)surrogate;
   return surrogateCall(s, [&]() {
     requireDevice(points, "points");
+    s->checkTimeout();
     cudaStream_t st = s->device->stream;
     cudaCheck(cudaMemsetAsync(s->regionErr.ptr, 0, s->numRegions * 4, st), "memset");
     cudaCheck(cudaMemsetAsync(s->regionSeen.ptr, 0, s->numRegions * 4, st), "memset");
@@ -898,6 +1063,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateCalibrate(VKLCudaSurr
     unsigned int f = 0;
     cudaCheck(cudaMemcpyAsync(&f, s->scalars.ptr, 4, cudaMemcpyDeviceToHost, st), "copy");
     cudaCheck(cudaStreamSynchronize(st), "surrogate calibration");
+    s->checkTimeout();
     if (flaggedRegions)
       *flaggedRegions = f;
   });
@@ -911,6 +1077,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateSample(VKLCudaSurroga
   return surrogateCall(s, [&]() {
     requireDevice(points, "points");
     requireDevice(samples, "samples");
+    s->checkTimeout();
     if (n)
       s->infer<0>(n, (const float *)points, samples, fallback, s->device->stream);
   });
