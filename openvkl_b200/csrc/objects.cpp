@@ -434,7 +434,9 @@ namespace {
 
 // Planes per atlas row for X x Y x Z float planes within the device's 2D
 // texture and surface limits; 0 when the volume does not fit one atlas.
-// Up to 64 planes side by side keep z-neighbours a few KB apart.
+// Up to 64 planes side by side keep z-neighbours a few KB apart.  The count
+// is a power of two, so the sampling kernels find a plane's tile with a
+// shift and a mask instead of an integer division.
 uint32_t atlasPlanesPerRow(int cudaDevice, uint32_t X, uint32_t Y, uint32_t Z)
 {
   int tw = 0, th = 0, sw = 0, sh = 0;
@@ -443,16 +445,15 @@ uint32_t atlasPlanesPerRow(int cudaDevice, uint32_t X, uint32_t Y, uint32_t Z)
   cudaDeviceGetAttribute(&sw, cudaDevAttrMaxSurface2DWidth, cudaDevice);
   cudaDeviceGetAttribute(&sh, cudaDevAttrMaxSurface2DHeight, cudaDevice);
   const uint64_t maxW = (uint64_t)std::min(tw, sw), maxH = (uint64_t)std::min(th, sh);
-  uint64_t T = std::min<uint64_t>(Z, 64);
-  if (T * X > maxW)
-    T = maxW / X;
-  if (T == 0)
+  if (X == 0 || Y == 0 || Z == 0 || X > maxW)
     return 0;
-  if ((Z + T - 1) / T * Y > maxH) {
-    const uint64_t rowsMax = maxH / Y;
-    if (rowsMax == 0)
-      return 0;
-    T = (Z + rowsMax - 1) / rowsMax;
+  // the widest power of two up to 64 planes that fits the width and Z
+  uint64_t T = 64;
+  while (T > 1 && (T > Z || T * X > maxW))
+    T >>= 1;
+  // more planes per row when the rows would exceed the height
+  while ((Z + T - 1) / T * Y > maxH) {
+    T <<= 1;
     if (T * X > maxW)
       return 0;
   }

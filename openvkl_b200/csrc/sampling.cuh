@@ -344,7 +344,7 @@ struct AtlasField {
   uint64_t tex;
   uint32_t ax, ay, az;
   int32_t rx, ry, rz;
-  uint32_t planesPerRow;
+  uint32_t planeMask, planeShift;  // planes per atlas row (a power of two) - 1, log2
   float bg;
 
   __device__ __forceinline__ AtlasField(const DevGrid &g, uint32_t a)
@@ -355,9 +355,12 @@ struct AtlasField {
         rx(g.rootOrigin[0]),
         ry(g.rootOrigin[1]),
         rz(g.rootOrigin[2]),
-        planesPerRow(g.atlasPlanesPerRow),
+        planeMask(g.atlasPlanesPerRow - 1u),
+        planeShift(0u),
         bg(g.background[a])
   {
+    while ((1u << planeShift) < g.atlasPlanesPerRow)
+      ++planeShift;
   }
 
   __device__ __forceinline__ void corners(int32_t x, int32_t y, int32_t z, float s[8]) const
@@ -369,8 +372,8 @@ struct AtlasField {
     // (-1, -1) relative (only the +1 corner can be in the domain then)
     const float fx = vx0 ? (float)(ox + 1u) : 0.f, fy = vy0 ? (float)(oy + 1u) : 0.f;
     const uint32_t z0 = vz0 ? oz : 0u, z1 = vz1 ? oz + 1u : 0u;
-    const float4 a = tld4Red(tex, (float)((z0 % planesPerRow) * ax) + fx, (float)((z0 / planesPerRow) * ay) + fy);
-    const float4 b = tld4Red(tex, (float)((z1 % planesPerRow) * ax) + fx, (float)((z1 / planesPerRow) * ay) + fy);
+    const float4 a = tld4Red(tex, (float)((z0 & planeMask) * ax) + fx, (float)((z0 >> planeShift) * ay) + fy);
+    const float4 b = tld4Red(tex, (float)((z1 & planeMask) * ax) + fx, (float)((z1 >> planeShift) * ay) + fy);
     s[0] = (vx0 & vy0 & vz0) ? a.w : bg;
     s[1] = (vx0 & vy0 & vz1) ? b.w : bg;
     s[2] = (vx0 & vy1 & vz0) ? a.x : bg;
