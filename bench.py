@@ -1119,12 +1119,16 @@ def main(argv=None):
     ap.add_argument("--small", action="store_true",
                     help="512^3 volume, 480x270 rays x 256 (vdb: 2048^3 domain, 2^24 points): "
                          "the ncu capture case")
+    ap.add_argument("--volume-edge", type=int, default=0,
+                    help="edge of the dense volume instead of 1024 (512 with --small), the rays "
+                         "scaled to it: e.g. 128 for an L2-resident volume, the kernels' ceiling")
     args = ap.parse_args(argv)
+    global DIMS, WIDTH, HEIGHT, INCOHERENT_N, VDB_DOMAIN, VDB_POINTS, HIT_RAYS, TRAIN_STEPS
     if args.small:
-        global DIMS, WIDTH, HEIGHT, INCOHERENT_N, VDB_DOMAIN, VDB_POINTS, HIT_RAYS
         DIMS, WIDTH, HEIGHT, INCOHERENT_N = (512, 512, 512), 480, 270, 1 << 24
-        global TRAIN_STEPS
         VDB_DOMAIN, VDB_POINTS, HIT_RAYS, TRAIN_STEPS = 2048, 1 << 24, 1 << 20, 64
+    if args.volume_edge:
+        DIMS = (args.volume_edge,) * 3
     if args.no_extras:
         args.no_cpu_baseline = True
         args.no_patterns = True

@@ -40,8 +40,11 @@
 namespace vklcuda {
 namespace device_api {
 
+// The iterators' state lives in the caller's buffer (local memory of the
+// calling thread), so both use the DDA form indexed by the level at run time:
+// one copy of its step code per call site instead of one per tree level.
 struct IntervalIteratorState {
-  IntervalIt it;
+  IntervalItDyn it;
   const DevIntervalContextState *ctx;
 };
 struct HitIteratorState {

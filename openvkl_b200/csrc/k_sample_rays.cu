@@ -33,6 +33,7 @@ namespace {
 
 constexpr int kRunThreads = 256;
 constexpr int kRuns       = 8;  // runs per tile
+constexpr int kRunGroup   = 4;  // samples computed before their stores
 
 __device__ __forceinline__ uint32_t smemAddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -112,13 +113,18 @@ __global__ void __launch_bounds__(kRunThreads, runMinBlocks<Field>())
   // consecutive samples, 8 segments of 16 B (48 B for gradients).  Staging
   // them in shared memory between the samples (the rows share one array)
   // kept the compiler from overlapping consecutive samples' gathers: 7.85 vs
-  // 3.57 ms on the 1024^3 coherent workload.
+  // 3.57 ms on the 1024^3 coherent workload.  kRunGroup samples are computed
+  // before their stores, so their gathers are in flight together; points
+  // past the end of the array (zero rows of a partial tile) are computed
+  // and not stored.
+  constexpr int G = kRunGroup < PPT ? kRunGroup : PPT;
 #pragma unroll
-  for (int j = 0; j < PPT; ++j) {
-    const int k      = threadIdx.x + j * kRunThreads;
-    const int r      = k & (kRuns - 1), s = k >> 3;
-    const uint64_t i = base + (uint64_t)r * S + s;
-    if (i < n) {
+  for (int j0 = 0; j0 < PPT; j0 += G) {
+    float res[G][GRAD ? 3 : 1];
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int k    = threadIdx.x + (j0 + u) * kRunThreads;
+      const int r    = k & (kRuns - 1), s = k >> 3;
       const float *q = rows + r * L::kPtPitch + 3 * s;
       const f3 p     = xfmPoint(g.objectToIndex, f3{q[0], q[1], q[2]});
       if constexpr (GRAD) {
@@ -127,11 +133,26 @@ __global__ void __launch_bounds__(kRunThreads, runMinBlocks<Field>())
           gr = xfmNormal(g.objectToIndex, gradientCubic(F, p));
         else if constexpr (FILTER == kFilterLinear)
           gr = xfmNormal(g.objectToIndex, gradientLinear(F, p));
-        __stcs(out + 3 * i, gr.x);
-        __stcs(out + 3 * i + 1, gr.y);
-        __stcs(out + 3 * i + 2, gr.z);
+        res[u][0] = gr.x;
+        res[u][GRAD ? 1 : 0] = gr.y;
+        res[u][GRAD ? 2 : 0] = gr.z;
       } else {
-        __stcs(out + i, filterAt<Field, FILTER>(F, cc, p));
+        res[u][0] = filterAt<Field, FILTER>(F, cc, p);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int k      = threadIdx.x + (j0 + u) * kRunThreads;
+      const int r      = k & (kRuns - 1), s = k >> 3;
+      const uint64_t i = base + (uint64_t)r * S + s;
+      if (i < n) {
+        if constexpr (GRAD) {
+          __stcs(out + 3 * i, res[u][0]);
+          __stcs(out + 3 * i + 1, res[u][GRAD ? 1 : 0]);
+          __stcs(out + 3 * i + 2, res[u][GRAD ? 2 : 0]);
+        } else {
+          __stcs(out + i, res[u][0]);
+        }
       }
     }
   }
