@@ -3,25 +3,25 @@
 // A multi-resolution hash-grid encoding (16 levels, 2 FP16 features per
 // entry, per-level resolution floor(base * growth^l), direct indexing while
 // (res+1)^3 fits the table, else the spatial hash) feeds a 32-64-64-64-1 ReLU
-// MLP without biases, FP16 weights and activations on the tensor cores
-// (mma.sync m16n8k16, FP32 accumulation).  It is trained on samples of the
-// plain sampler (the caller supplies points and the plain samples as
-// targets), with the loss sum (y - target)^2 / n over the points with a
-// finite target, and Adam.  The plain sampler
-// also measures the error: calibration evaluates both on caller-supplied points
+// MLP without biases, FP16 weights and activations, FP32 accumulation.  It
+// is trained on samples of the plain sampler (the caller supplies points and
+// the plain samples as targets), with the loss sum (y - target)^2 / n over
+// the points with a finite target, and Adam.  The plain sampler also
+// measures the error: calibration evaluates both on caller-supplied points
 // and flags every 32^3-voxel region whose largest error exceeds a threshold
 // (or that no calibration point reached); sampling with fallback returns the
 // plain sample there and outside the volume's domain.
 //
-// Inference fuses the encoding and the MLP: a CTA encodes 128 points into
-// shared memory, each warp runs 32 of them through the MLP with the
-// activations kept in registers (an m16n8 accumulator tile is, after ReLU and
-// FP16 packing, exactly the A fragment of the next layer's m16n8k16 step).
-// Training runs forward and backward per 128-point tile in one kernel:
-// weight gradients as tensor-core products of the stored activations and
-// backward signals over the tile's points, encoding gradients scattered into
-// the table's gradient with float2 atomics; a separate kernel applies Adam to
-// the FP32 master parameters and refreshes their FP16 copies.
+// Inference fuses the encoding and the MLP: each 128-point group encodes its
+// points into shared memory and runs every hidden layer as one tcgen05
+// product (M = 128 points, N = 64) into tensor memory.  Training runs
+// forward and backward per 128-point tile in one kernel: forward and the
+// backward signals on mma.sync m16n8k16 tiles with the activations in
+// registers, the weight gradients (G^T H over the tile's points) as tcgen05
+// products from transposed, swizzled copies of the activations and signals,
+// encoding gradients scattered into the table's gradient with float2
+// atomics; a separate kernel applies Adam to the FP32 master parameters and
+// refreshes their FP16 copies.
 #include <cuda_fp16.h>
 
 #include <atomic>
@@ -221,11 +221,24 @@ __device__ __forceinline__ void loadFwdWeights(FwdWeights &W, const __half *__re
     W.w4[k / kH][k % kH] = k < kH ? w16[kOffW4 + k] : __float2half(0.f);
 }
 
+// Transposed operands of the training kernel's tensor-core weight gradients
+// (dW = G^T H over a tile's 128 points): unit u is a row, point p the K
+// index, in the 128-byte-swizzled K-major layout (tcgen05.cuh), as two atoms
+// of 64 points; an atom holds `rows` rows of 128 bytes.  Byte offset of
+// element (u, p):
+__device__ __forceinline__ uint32_t tOff(uint32_t rows, uint32_t u, uint32_t p)
+{
+  return (p >> 6) * (rows * 128u) + tc::swizzledChunk(u, (p & 63u) >> 3) + (p & 7u) * 2u;
+}
+constexpr uint32_t kTBytes64 = 2 * 64 * 128;  // 64 units x 128 points
+constexpr uint32_t kTBytes32 = 2 * 32 * 128;  // 32 units x 128 points
+
 // Forward of one 16-row chunk (rows m0..m0+15 of X); returns the outputs of
 // rows m0+g and m0+g+8 in lanes with t == 0.  When HT is given, the FP16
-// activations of each hidden layer are also stored transposed: HT[l][col][row].
+// activations of each hidden layer l are also stored transposed at
+// HT + l * kTBytes64 (tOff layout).
 __device__ __forceinline__ void forwardChunk(const FwdWeights &W, const __half *X, int ldx, int m0, int g, int t,
-                                             float &y0, float &y1, __half *HT, int ldh)
+                                             float &y0, float &y1, unsigned char *HT)
 {
   uint32_t a[4][4];
   float acc[8][4];
@@ -247,16 +260,16 @@ __device__ __forceinline__ void forwardChunk(const FwdWeights &W, const __half *
   for (int layer = 0; layer < 3; ++layer) {
     chain(acc, a);
     if (HT) {
-      __half *H = HT + (size_t)layer * kH * ldh;
+      unsigned char *H = HT + (size_t)layer * kTBytes64;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int c = 8 * j + 2 * t;
         const __half2 lo = *reinterpret_cast<const __half2 *>(&a[j >> 1][(j & 1) ? 2 : 0]);
         const __half2 hi = *reinterpret_cast<const __half2 *>(&a[j >> 1][(j & 1) ? 3 : 1]);
-        H[c * ldh + m0 + g]           = __low2half(lo);
-        H[(c + 1) * ldh + m0 + g]     = __high2half(lo);
-        H[c * ldh + m0 + g + 8]       = __low2half(hi);
-        H[(c + 1) * ldh + m0 + g + 8] = __high2half(hi);
+        *reinterpret_cast<__half *>(H + tOff(64, c, m0 + g))         = __low2half(lo);
+        *reinterpret_cast<__half *>(H + tOff(64, c + 1, m0 + g))     = __high2half(lo);
+        *reinterpret_cast<__half *>(H + tOff(64, c, m0 + g + 8))     = __low2half(hi);
+        *reinterpret_cast<__half *>(H + tOff(64, c + 1, m0 + g + 8)) = __high2half(hi);
       }
     }
     if (layer == 2)
@@ -315,6 +328,7 @@ struct TcInferSmem {                // operand buffers on 1024-byte boundaries
   uint32_t tmem;
 };
 constexpr size_t kTcInferSmemBytes = sizeof(TcInferSmem) + 1024;  // + alignment slack
+static_assert(kInferCtasPerSM * (kTcInferSmemBytes + 1024) <= 228 * 1024, "inference CTAs per SM exceed shared memory");
 
 // Rows of a row-major [rows][k] FP16 matrix into the swizzled K-major layout.
 __device__ __forceinline__ void loadSwizzledRows(unsigned char *dst, const __half *__restrict__ src, int rows, int k)
@@ -493,53 +507,73 @@ __global__ void kRegionFlags(uint64_t n, const float *regionErr, const uint32_t 
 // ---------------------------------------------------------------------------
 // Training: forward + backward of 128-point tiles.
 // ---------------------------------------------------------------------------
-constexpr int kLdT = kTile + 8;  // transposed buffers: [col][row]
 constexpr int kLdR = kH + 8;     // row-major [row][64]
 
-struct TrainSmem {
+struct TrainSmem {  // GT, HT, XT on 1024-byte boundaries (the struct is placed so)
+  unsigned char GT[kTBytes64];     // backward signal, transposed (A of the weight gradients)
+  unsigned char HT[3][kTBytes64];  // hidden activations, transposed (B)
+  unsigned char XT[kTBytes32];     // encoded inputs, transposed (B of dW1)
   FwdWeights W;
   __half w1t[kIn][kH + 8];   // W1 transposed [in][out]
   __half w2t[kH][kH + 8];
   __half w3t[kH][kH + 8];
   float w4[kH];
   __half X[kTile][kIn + 8];
-  __half XT[kIn][kLdT];
-  __half HT[3][kH][kLdT];    // hidden activations, transposed
   __half G[kTile][kLdR];     // backward signal, row-major
-  __half GT[kH][kLdT];       // and transposed
   float u[kTile][3];
   float dy[kTile];
   float loss[kThr / 32];
+  uint64_t bar;
+  uint32_t tmem;
 };
+constexpr size_t kTrainSmemBytes = sizeof(TrainSmem) + 1024;  // + alignment slack
+constexpr uint32_t kTrainCols    = 64;                         // TMEM columns: one 64-wide accumulator
+static_assert(kTrainSmemBytes <= 227 * 1024, "training tile exceeds the shared memory of one CTA");
 
-// dW (64 x N) += GT (64 x 128) * BT (N x 128)^T for output rows 16w..16w+15.
-template <int NT>
-__device__ __forceinline__ void weightGrad(const TrainSmem &S, const __half *BT, int warp, int g, int t,
-                                           float *__restrict__ gW, int ldw)
+// Weight gradient dW (64 x N) += G^T (64 x 128 points) * B^T on the tensor
+// cores: one thread issues 8 K-steps of M = 128 (rows 64..127 of the A
+// operand read the next 8 KB of shared memory and land in TMEM lanes
+// 64..127, which nobody reads), N = 64 or 32, then every thread waits for the
+// commit; warps 0 and 1 read lanes 0..63 (output units) and add them to the
+// FP32 gradient in global memory.  Returns false if the wait gave up.
+template <int N>
+__device__ __forceinline__ bool weightGradTc(TrainSmem &S, const unsigned char *B, uint32_t &phase,
+                                             float *__restrict__ gW)
 {
-  float acc[NT][4];
+  constexpr uint32_t idesc = tc::f16InstrDesc(128, N);
+  const uint32_t aBase = tc::smemAddr(S.GT), bBase = tc::smemAddr(B);
+  if (threadIdx.x == 0) {
+    tc::fenceAfterSync();
 #pragma unroll
-  for (int j = 0; j < NT; ++j)
-    acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    for (int k = 0; k < kTile / 16; ++k) {
+      const uint32_t off = (uint32_t)(k >> 2), in = 32u * (uint32_t)(k & 3);
+      tc::mmaF16(S.tmem, tc::sw128Desc(aBase + off * (64u * 128u) + in),
+                 tc::sw128Desc(bBase + off * ((uint32_t)N * 128u) + in), idesc, k > 0);
+    }
+    tc::commitTo(&S.bar);
+  }
+  const bool done = tc::mbarWait(&S.bar, phase);
+  phase ^= 1u;
+  if (__syncthreads_or(!done))
+    return false;
+  tc::fenceAfterSync();
+  const int warp = threadIdx.x >> 5;
+  if (warp < 2) {
+    const uint32_t o = threadIdx.x;  // output unit = TMEM lane
 #pragma unroll
-  for (int kk = 0; kk < kTile / 16; ++kk) {
-    uint32_t a[4];
-    loadA(a, &S.GT[0][0], kLdT, 16 * warp, 16 * kk, g, t);
+    for (int h = 0; h < N / 32; ++h) {
+      uint32_t r[32];
+      tc::tmemLoad32(S.tmem + ((uint32_t)(32 * warp) << 16) + 32u * h, r);
+      tc::tmemLoadWait();
+      float4 *dst = reinterpret_cast<float4 *>(gW + (size_t)o * N + 32 * h);
 #pragma unroll
-    for (int j = 0; j < NT; ++j) {
-      uint32_t b0, b1;
-      loadB(b0, b1, BT, kLdT, 8 * j, 16 * kk, g, t);
-      mma16816(acc[j], a, b0, b1);
+      for (int q = 0; q < 8; ++q)
+        atomicAdd(dst + q, make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                       __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3])));
     }
   }
-#pragma unroll
-  for (int j = 0; j < NT; ++j) {
-    const int r = 16 * warp + g, c = 8 * j + 2 * t;
-    atomicAdd(gW + r * ldw + c, acc[j][0]);
-    atomicAdd(gW + r * ldw + c + 1, acc[j][1]);
-    atomicAdd(gW + (r + 8) * ldw + c, acc[j][2]);
-    atomicAdd(gW + (r + 8) * ldw + c + 1, acc[j][3]);
-  }
+  tc::fenceBeforeSync();
+  return true;
 }
 
 // Backward signal of the previous layer for this warp's 32 rows:
@@ -567,26 +601,27 @@ __device__ __forceinline__ void signalGrad(const TrainSmem &S, const __half *Wt,
   }
 }
 
-// G <- ReLU-masked signal (mask from the stored activations HT[col][row]).
-__device__ __forceinline__ void storeSignal(TrainSmem &S, const float acc[2][8][4], const __half *H, int warp,
-                                            int g, int t)
+// G <- ReLU-masked signal (mask from the stored transposed activations H).
+__device__ __forceinline__ void storeSignal(TrainSmem &S, const float acc[2][8][4], const unsigned char *H,
+                                            int warp, int g, int t)
 {
 #pragma unroll
   for (int c = 0; c < 2; ++c)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int r = 32 * warp + 16 * c + g, col = 8 * j + 2 * t;
-      const float v0 = __half2float(H[col * kLdT + r]) > 0.f ? acc[c][j][0] : 0.f;
-      const float v1 = __half2float(H[(col + 1) * kLdT + r]) > 0.f ? acc[c][j][1] : 0.f;
-      const float v2 = __half2float(H[col * kLdT + r + 8]) > 0.f ? acc[c][j][2] : 0.f;
-      const float v3 = __half2float(H[(col + 1) * kLdT + r + 8]) > 0.f ? acc[c][j][3] : 0.f;
+      auto hv = [&](int u, int p) { return __half2float(*reinterpret_cast<const __half *>(H + tOff(64, u, p))); };
+      const float v0 = hv(col, r) > 0.f ? acc[c][j][0] : 0.f;
+      const float v1 = hv(col + 1, r) > 0.f ? acc[c][j][1] : 0.f;
+      const float v2 = hv(col, r + 8) > 0.f ? acc[c][j][2] : 0.f;
+      const float v3 = hv(col + 1, r + 8) > 0.f ? acc[c][j][3] : 0.f;
       const __half2 lo = __floats2half2_rn(v0, v1), hi = __floats2half2_rn(v2, v3);
       *reinterpret_cast<__half2 *>(&S.G[r][col])     = lo;
       *reinterpret_cast<__half2 *>(&S.G[r + 8][col]) = hi;
-      S.GT[col][r]         = __low2half(lo);
-      S.GT[col + 1][r]     = __high2half(lo);
-      S.GT[col][r + 8]     = __low2half(hi);
-      S.GT[col + 1][r + 8] = __high2half(hi);
+      *reinterpret_cast<__half *>(S.GT + tOff(64, col, r))         = __low2half(lo);
+      *reinterpret_cast<__half *>(S.GT + tOff(64, col + 1, r))     = __high2half(lo);
+      *reinterpret_cast<__half *>(S.GT + tOff(64, col, r + 8))     = __low2half(hi);
+      *reinterpret_cast<__half *>(S.GT + tOff(64, col + 1, r + 8)) = __high2half(hi);
     }
 }
 
@@ -596,10 +631,10 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
                                                         const float *__restrict__ pts,
                                                         const float *__restrict__ targets,
                                                         float2 *__restrict__ gTable, float *__restrict__ gW,
-                                                        float *__restrict__ lossOut)
+                                                        float *__restrict__ lossOut, uint32_t *__restrict__ err)
 {
-  extern __shared__ __align__(16) unsigned char smemRaw[];
-  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smemRaw);
+  extern __shared__ unsigned char smemRaw[];
+  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smemRaw + ((1024u - (tc::smemAddr(smemRaw) & 1023u)) & 1023u));
   loadFwdWeights(S.W, w16);
   for (int k = threadIdx.x; k < kH * kIn; k += kThr)
     S.w1t[k % kIn][k / kIn] = w16[kOffW1 + k];
@@ -610,8 +645,17 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
   for (int k = threadIdx.x; k < kH; k += kThr)
     S.w4[k] = __half2float(w16[kOffW4 + k]);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  if (threadIdx.x == 0)
+    tc::mbarInit(&S.bar, 1);
+  if (warp == 0)
+    tc::tmemAlloc(&S.tmem, kTrainCols);
+  tc::fenceBeforeSync();
+  __syncthreads();
+  tc::fenceAfterSync();
+  uint32_t phase = 0;
+  bool ok        = true;
   float lossAcc = 0.f;
-  for (uint64_t base = (uint64_t)blockIdx.x * kTile; base < n; base += (uint64_t)gridDim.x * kTile) {
+  for (uint64_t base = (uint64_t)blockIdx.x * kTile; base < n && ok; base += (uint64_t)gridDim.x * kTile) {
     const uint64_t i = base + threadIdx.x;
     float u[3]       = {0.f, 0.f, 0.f};
     __half2 *row     = reinterpret_cast<__half2 *>(&S.X[threadIdx.x][0]);
@@ -628,13 +672,13 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
     S.u[threadIdx.x][2] = u[2];
     __syncthreads();
     for (int k = 0; k < kIn; ++k)
-      S.XT[k][threadIdx.x] = S.X[threadIdx.x][k];
+      *reinterpret_cast<__half *>(S.XT + tOff(32, k, threadIdx.x)) = S.X[threadIdx.x][k];
     // forward; output and d(loss)/dy per row
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const int m0 = 32 * warp + 16 * c;
       float y0, y1;
-      forwardChunk(S.W, &S.X[0][0], kIn + 8, m0, g, t, y0, y1, &S.HT[0][0][0], kLdT);
+      forwardChunk(S.W, &S.X[0][0], kIn + 8, m0, g, t, y0, y1, &S.HT[0][0]);
       if (t == 0) {
         const uint64_t r0 = base + m0 + g, r1 = r0 + 8;
         // points whose target is not finite (outside the data, where a
@@ -649,34 +693,49 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
     }
     __syncthreads();
     // layer 4: dW4 and the signal into layer 3
+    auto ht = [&](int l, int u, int p) {
+      return __half2float(*reinterpret_cast<const __half *>(S.HT[l] + tOff(64, u, p)));
+    };
     if (threadIdx.x < kH) {
       float s = 0.f;
       for (int r = 0; r < kTile; ++r)
-        s += S.dy[r] * __half2float(S.HT[2][threadIdx.x][r]);
+        s += S.dy[r] * ht(2, threadIdx.x, r);
       atomicAdd(gW + kOffW4 + threadIdx.x, s);
     }
     {
       const int r = threadIdx.x;
       for (int col = 0; col < kH; ++col) {
-        const float v = __half2float(S.HT[2][col][r]) > 0.f ? S.dy[r] * S.w4[col] : 0.f;
+        const float v = ht(2, col, r) > 0.f ? S.dy[r] * S.w4[col] : 0.f;
         const __half h = __float2half_rn(v);
-        S.G[r][col]  = h;
-        S.GT[col][r] = h;
+        S.G[r][col] = h;
+        *reinterpret_cast<__half *>(S.GT + tOff(64, col, r)) = h;
       }
     }
+    // the transposed operands are read by the tensor cores (async proxy)
+    tc::fenceProxyAsync();
+    tc::fenceBeforeSync();
     __syncthreads();
-    // layers 3 and 2: weight gradient, then the signal into the layer below
+    // layers 3 and 2: weight gradient (tensor cores) beside the signal into
+    // the layer below (mma.sync), then the new signal
 #pragma unroll 1
-    for (int layer = 2; layer >= 1; --layer) {
-      weightGrad<8>(S, &S.HT[layer - 1][0][0], warp, g, t, gW + (layer == 2 ? kOffW3 : kOffW2), kH);
+    for (int layer = 2; layer >= 1 && ok; --layer) {
       float acc[2][8][4];
       signalGrad<8>(S, layer == 2 ? &S.w3t[0][0] : &S.w2t[0][0], warp, g, t, acc);
+      ok = weightGradTc<64>(S, S.HT[layer - 1], phase, gW + (layer == 2 ? kOffW3 : kOffW2));
+      if (!ok)
+        break;
       __syncthreads();
-      storeSignal(S, acc, &S.HT[layer - 1][0][0], warp, g, t);
+      storeSignal(S, acc, S.HT[layer - 1], warp, g, t);
+      tc::fenceProxyAsync();
+      tc::fenceBeforeSync();
       __syncthreads();
     }
+    if (!ok)
+      break;
     // layer 1: weight gradient and the encoding gradient
-    weightGrad<4>(S, &S.XT[0][0], warp, g, t, gW + kOffW1, kIn);
+    ok = weightGradTc<kIn>(S, S.XT, phase, gW + kOffW1);
+    if (!ok)
+      break;
     {
       float acc[2][4][4];
       signalGrad<4>(S, &S.w1t[0][0], warp, g, t, acc);
@@ -707,6 +766,12 @@ __global__ void __launch_bounds__(kThr) kSurrogateTrain(const __grid_constant__ 
     }
     __syncthreads();  // shared buffers are reused by the next tile
   }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (warp == 0)
+    tc::tmemDealloc(S.tmem, kTrainCols);
+  if (!ok && threadIdx.x == 0)
+    atomicExch(err, 1u);
   // loss of this CTA
   for (int o = 16; o > 0; o >>= 1)
     lossAcc += __shfl_xor_sync(0xffffffffu, lossAcc, o);
@@ -783,16 +848,20 @@ struct Surrogate {
 
   void train(uint64_t n, const float *pts, const float *targets, float *lossDev, cudaStream_t st)
   {
-    static bool attrSet = false;
-    if (!attrSet) {
+    // the dynamic shared-memory limit is raised once per device (bit = ordinal)
+    static std::atomic<uint64_t> configured{0};
+    const uint64_t bit = 1ull << (device->cudaDevice & 63);
+    if (!(configured.load() & bit)) {
       cudaCheck(cudaFuncSetAttribute(kSurrogateTrain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(TrainSmem)),
+                                     (int)kTrainSmemBytes),
                 "smem attribute");
-      attrSet = true;
+      configured.fetch_or(bit);
     }
-    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, kTile), (uint64_t)numSMs * 8);
-    kSurrogateTrain<<<grid, kThr, sizeof(TrainSmem), st>>>(E, table16.as<__half2>(), w16.as<__half>(), n, pts,
-                                                           targets, gTable.as<float2>(), gW.as<float>(), lossDev);
+    // one CTA per SM fits (the tile's activations, signals and weights)
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks(n, kTile), (uint64_t)numSMs);
+    kSurrogateTrain<<<grid, kThr, kTrainSmemBytes, st>>>(E, table16.as<__half2>(), w16.as<__half>(), n, pts,
+                                                         targets, gTable.as<float2>(), gW.as<float>(), lossDev,
+                                                         errDev);
     cudaCheck(cudaGetLastError(), "surrogate train kernel");
   }
 
@@ -838,13 +907,13 @@ struct Surrogate {
       inferWith<SparseField<float>, MODE>(n, pts, out, fallback, st);
   }
 
-  // A tensor-core wait of an earlier inference launch that gave up sets a
-  // word of host-mapped memory; the next call reports it.
+  // A tensor-core wait of an earlier inference or training launch that gave
+  // up sets a word of host-mapped memory; the next call reports it.
   void checkTimeout()
   {
     if (errHost && *(volatile uint32_t *)errHost) {
       *(volatile uint32_t *)errHost = 0u;
-      fail("surrogate: a tensor-core completion wait of an earlier inference launch timed out", VKL_UNKNOWN_ERROR);
+      fail("surrogate: a tensor-core completion wait of an earlier launch timed out", VKL_UNKNOWN_ERROR);
     }
   }
 
@@ -1008,6 +1077,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGradient(VKLCudaSurro
   return surrogateCall(s, [&]() {
     requireDevice(points, "points");
     requireDevice(targets, "targets");
+    s->checkTimeout();
     cudaStream_t st = s->device->stream;
     s->zeroGrads(st);
     cudaCheck(cudaMemsetAsync(s->scalars.ptr, 0, 4, st), "memset");
@@ -1019,6 +1089,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateGradient(VKLCudaSurro
     if (weightGrad)
       cudaCheck(cudaMemcpyAsync(weightGrad, s->gW.ptr, kNumW * 4, cudaMemcpyDefault, st), "copy");
     cudaCheck(cudaStreamSynchronize(st), "surrogate gradient");
+    s->checkTimeout();
     s->zeroGrads(st);
   });
 }
@@ -1031,6 +1102,7 @@ extern "C" OPENVKL_CUDA_INTERFACE VKLError vklCudaSurrogateTrainStep(VKLCudaSurr
   return surrogateCall(s, [&]() {
     requireDevice(points, "points");
     requireDevice(targets, "targets");
+    s->checkTimeout();
     if (n == 0)
       return;
     cudaStream_t st = s->device->stream;
