@@ -403,7 +403,9 @@ def run_cuda(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg, "compulsory_voxel_bytes": comp},
-            "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps,
+            # per step: the layout detection (kDetectRuns) and the sampling
+            # kernel for trilinear calls; the sampling kernel alone for tricubic
+            "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps * (1 if f == 200 else 2),
             "clocks": clocks,
         }
         if patterns is not None:
