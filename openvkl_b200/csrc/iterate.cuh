@@ -776,15 +776,20 @@ enum HitPhase : int {
   kHpDone
 };
 
-template <class Hook>
+// Rays: the lane's ray source.  rays.next(h, out) starts the lane's next ray
+// (hitInit into h, out = its first hit slot) and returns false when the lane
+// has none left; rays.finish(count) records the hit count of the ray just
+// completed.  A lane that finishes a ray starts its next one within the same
+// warp iteration, so a warp does not idle behind its longest ray.
+template <class Hook, class Rays>
 __device__ inline void hitsAllLanes(const DevGrid &g, const Hook &hook, uint32_t attr, const DevValueRanges &vr,
-                                    uint32_t numValues, const float *values, HitIt &h, bool active,
-                                    uint32_t maxPerRay, DevHit *out, uint32_t &count)
+                                    uint32_t numValues, const float *values, uint32_t maxPerRay, Rays &rays)
 {
-  const HitCtx<Hook> c{hook, h.o, h.d};
-  const float dlen = sqrtf(h.d.x * h.d.x + h.d.y * h.d.y + h.d.z * h.d.z);
-  int ph    = active ? kHpTop : kHpDone;
-  count     = 0;
+  HitIt h;
+  DevHit *out    = nullptr;
+  uint32_t count = 0;
+  int ph         = rays.next(h, out) ? kHpTop : kHpDone;
+  float dlen     = sqrtf(h.d.x * h.d.x + h.d.y * h.d.y + h.d.z * h.d.z);
   // intersectBisection state
   float t0 = 0.f, s0 = 0.f, tHi = 0.f, step = 0.f, hs = 0.f, t = 0.f, s = 0.f, ts = 0.f;
   uint32_t march = 0;
@@ -992,11 +997,19 @@ __device__ inline void hitsAllLanes(const DevGrid &g, const Hook &hook, uint32_t
         ph = kHpDone;
         break;
       }
+      if (ph == kHpDone) {  // the ray is complete: record it, start the next
+        rays.finish(count);
+        if (rays.next(h, out)) {
+          count = 0;
+          dlen  = sqrtf(h.d.x * h.d.x + h.d.y * h.d.y + h.d.z * h.d.z);
+          ph    = kHpTop;
+        }
+      }
     }
     if (!__any_sync(0xffffffffu, want))
       return;
     if (want)
-      sample = c.sampleAt(tReq);
+      sample = hook({h.o.x + tReq * h.d.x, h.o.y + tReq * h.d.y, h.o.z + tReq * h.d.z});
   }
 }
 

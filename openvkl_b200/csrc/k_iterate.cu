@@ -2,6 +2,8 @@
 // ray through the whole DDA / hit loop; the per-call forms back the C API's
 // stateful vklIterateInterval / vklIterateHit by advancing a state struct
 // that lives in the caller's buffer by one step.
+#include <algorithm>
+
 #include "iterate.cuh"
 #include "kernels.h"
 #include "objects.h"
@@ -47,6 +49,32 @@ __global__ void __launch_bounds__(kBlock, kIntervalMinBlocks) kIntervals(const _
   counts[r] = c;
 }
 
+// The ray source of the persistent hit kernels: rays first, first + stride,
+// ... below n, each with its slots out[r * maxPerRay ..] and count counts[r].
+struct StridedRays {
+  const DevGrid *g;
+  uint32_t depth;
+  uint64_t r, stride, n;
+  const float *orgs, *dirs, *tr;
+  DevHit *outBase;
+  uint32_t maxPerRay;
+  uint32_t *counts;
+  bool started = false;
+
+  __device__ __forceinline__ bool next(HitIt &h, DevHit *&out)
+  {
+    if (started)
+      r += stride;
+    started = true;
+    if (r >= n)
+      return false;
+    hitInit(*g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), h);
+    out = outBase + r * maxPerRay;
+    return true;
+  }
+  __device__ __forceinline__ void finish(uint32_t count) { counts[r] = count; }
+};
+
 // Field specialisations of the batched hit kernel: the generic one samples
 // through the out-of-line type / filter dispatch; the float trilinear ones
 // inline their field (far fewer registers, so more rays in flight per SM)
@@ -81,20 +109,17 @@ __global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid 
     }
     counts[r] = c;
   } else {
-    // every lane of the warp stays in the state machine's warp-wide loop
-    const bool active = r < n;
-    const uint64_t rr = active ? r : n - 1;
-    HitIt h;
-    hitInit(g, depth, ld3(orgs, rr), ld3(dirs, rr), __ldg(tr + 2 * rr), __ldg(tr + 2 * rr + 1), h);
-    uint32_t c = 0;
+    // Persistent: lane r takes rays r, r + stride, ... (stride = the grid's
+    // threads) and starts the next as soon as one is done.  Every lane of
+    // the warp stays in the state machine's warp-wide loop until all its
+    // lanes are out of rays.
+    StridedRays rays{&g, depth, r, (uint64_t)gridDim.x * kBlock, n, orgs, dirs, tr, out, maxPerRay, counts};
     if constexpr (KIND == kHitDenseFloatLinear)
       hitsAllLanes(g, LinearSampleHook<DenseField<float>>{&g, DenseField<float>(g, attr)}, attr, vr, numValues,
-                   values, h, active, maxPerRay, out + rr * maxPerRay, c);
+                   values, maxPerRay, rays);
     else
       hitsAllLanes(g, LinearSampleHook<SparseField<float>>{&g, SparseField<float>(g, attr, kNumLevels - 1)}, attr,
-                   vr, numValues, values, h, active, maxPerRay, out + rr * maxPerRay, c);
-    if (active)
-      counts[r] = c;
+                   vr, numValues, values, maxPerRay, rays);
   }
 }
 
@@ -169,12 +194,18 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
     return;
   const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && g.compress == kCompressNone && !g.temporal;
   auto k         = kHits<kHitAny, 1>;
-  if (lin && g.dense)
-    k = kHits<kHitDenseFloatLinear, kHitLookahead>;
-  else if (lin)
-    k = kHits<kHitSparseFloatLinear, kHitLookahead>;
-  k<<<blocksFor(n), kBlock, 0, st>>>(g, attr, filter, depth, vr, numValues, values, n, origins, directions,
-                                     tRanges, maxPerRay, out, counts);
+  unsigned grid  = blocksFor(n);
+  if (lin) {
+    k = g.dense ? kHits<kHitDenseFloatLinear, kHitLookahead> : kHits<kHitSparseFloatLinear, kHitLookahead>;
+    // persistent: as many CTAs as are resident at once
+    int dev = 0, sms = 0, perSM = 0;
+    cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, kBlock, 0), "occupancy");
+    grid = (unsigned)std::min<uint64_t>(grid, (uint64_t)sms * (uint64_t)std::max(perSM, 1));
+  }
+  k<<<grid, kBlock, 0, st>>>(g, attr, filter, depth, vr, numValues, values, n, origins, directions, tRanges,
+                             maxPerRay, out, counts);
   cudaCheck(cudaGetLastError(), "hit kernel launch");
 }
 
