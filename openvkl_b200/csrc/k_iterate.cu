@@ -18,6 +18,10 @@ constexpr int kBlock = 128;
 // workload): 4 x 128 threads (128 registers) ran fastest; 6 x 128 fits it in
 // 80 registers but ran 10 % slower.
 constexpr int kIntervalMinBlocks = 4;
+// The specialised (persistent) hit kernels run fastest at 6 x 128 threads per
+// SM (80 registers): 7.39 vs 6.86 Mrays/s at 5 (96 registers) on 2^24 random
+// rays through the 4096^3 shell VDB.
+constexpr int kHitMinBlocks = 6;
 
 __device__ __forceinline__ f3 ld3(const float *p, uint64_t i)
 {
@@ -83,7 +87,7 @@ enum HitKind { kHitAny = 0, kHitDenseFloatLinear = 1, kHitSparseFloatLinear = 2 
 constexpr int kHitLookahead = 1;
 
 template <int KIND, int LOOKAHEAD>
-__global__ void __launch_bounds__(kBlock) kHits(const __grid_constant__ DevGrid g, uint32_t attr,
+__global__ void __launch_bounds__(kBlock, KIND == kHitAny ? 1 : kHitMinBlocks) kHits(const __grid_constant__ DevGrid g, uint32_t attr,
                                                 int filter, uint32_t depth, DevValueRanges vr,
                                                 uint32_t numValues,
                                                 const float *__restrict__ values, uint64_t n,
