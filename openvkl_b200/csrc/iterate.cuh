@@ -270,21 +270,19 @@ __device__ __forceinline__ bool rangesOverlap(const DevValueRanges &vr, float lo
   return false;
 }
 
-__device__ inline void queryVoxelDense(const DevGrid &g, int32_t x, int32_t y, int32_t z,
-                                       uint32_t depth, uint32_t attr, const DevValueRanges &vr,
-                                       VoxelDesc &desc)
+// The value range of the dense tree's node voxel holding cell (x, y, z) at
+// the query depth, or null outside the domain.  The reference computes the
+// level-1/2 node numbers in closed form (VdbQueryVoxelDense.ih:41-113).  The
+// dense tree numbers level-l nodes x-fastest over the node grid (k_build.cu
+// kDenseLevel*), so the node of an in-domain cell is its node coordinates'
+// linear index: the same voxel the child-pointer walk reaches, without its
+// two dependent loads.
+__device__ __forceinline__ const float *denseCellRange(const DevGrid &g, int32_t x, int32_t y, int32_t z,
+                                                       uint32_t depth, uint32_t attr)
 {
-  desc.level = depth;
   const uint32_t ox = (uint32_t)x, oy = (uint32_t)y, oz = (uint32_t)z;
-  if (!(ox < g.activeSize[0] && oy < g.activeSize[1] && oz < g.activeSize[2])) {
-    desc.isEmpty = true;
-    return;
-  }
-  // The reference computes the level-1/2 node numbers in closed form
-  // (VdbQueryVoxelDense.ih:41-113).  The dense tree numbers level-l nodes
-  // x-fastest over the node grid (k_build.cu kDenseLevel*), so the node of
-  // an in-domain cell is its node coordinates' linear index: the same voxel
-  // the child-pointer walk reaches, without its two dependent loads.
+  if (!(ox < g.activeSize[0] && oy < g.activeSize[1] && oz < g.activeSize[2]))
+    return nullptr;
   const uint32_t lvl = depth >= 2 ? 2u : depth;
   uint64_t ni = offsetToLinear(lvl, ox, oy, oz);
   if (lvl == 2) {
@@ -294,10 +292,22 @@ __device__ inline void queryVoxelDense(const DevGrid &g, int32_t x, int32_t y, i
     const uint32_t n1x = (g.activeSize[0] + 4095) >> 12, n1y = (g.activeSize[1] + 4095) >> 12;
     ni += (((uint64_t)(oz >> 12) * n1y + (oy >> 12)) * n1x + (ox >> 12)) * levelNumVoxels(1);
   }
-  const float *r = g.levels[lvl].valueRange + 2 * (ni * g.numAttributes + attr);
-  desc.v0        = __ldg(r);
-  desc.v1        = __ldg(r + 1);
-  desc.isEmpty   = !rangesOverlap(vr, desc.v0, desc.v1);
+  return g.levels[lvl].valueRange + 2 * (ni * g.numAttributes + attr);
+}
+
+__device__ inline void queryVoxelDense(const DevGrid &g, int32_t x, int32_t y, int32_t z,
+                                       uint32_t depth, uint32_t attr, const DevValueRanges &vr,
+                                       VoxelDesc &desc)
+{
+  desc.level    = depth;
+  const float *r = denseCellRange(g, x, y, z, depth, attr);
+  if (!r) {
+    desc.isEmpty = true;
+    return;
+  }
+  desc.v0      = __ldg(r);
+  desc.v1      = __ldg(r + 1);
+  desc.isEmpty = !rangesOverlap(vr, desc.v0, desc.v1);
 }
 
 __device__ inline void queryVoxelSparse(const DevGrid &g, int32_t x, int32_t y, int32_t z,

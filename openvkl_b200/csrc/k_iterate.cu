@@ -53,6 +53,87 @@ __global__ void __launch_bounds__(kBlock, kIntervalMinBlocks) kIntervals(const _
   counts[r] = c;
 }
 
+// Dense volumes: a cell's query never changes the DDA's path (the node
+// level is always the query depth), so the steps can run ahead of the value
+// range loads.  Each round records up to kIntervalLookahead steps (cell
+// range address, t before and after the step, the budget), then loads their
+// ranges together and applies intervalNext's tests to them in order: a
+// non-empty cell whose t is not below tMax ends the ray, a spent budget ends
+// it without emitting, a non-empty cell emits [t before, min(t after,
+// tMax)].  Steps recorded past the end of a ray are dropped.  The intervals
+// are those of intervalNext, in the same order.
+constexpr int kIntervalLookahead = 8;
+
+__global__ void __launch_bounds__(kBlock, kIntervalMinBlocks)
+    kIntervalsDense(const __grid_constant__ DevGrid g, uint32_t attr, uint32_t depth, DevValueRanges vr, uint64_t n,
+                    const float *__restrict__ orgs, const float *__restrict__ dirs, const float *__restrict__ tr,
+                    uint32_t maxPerRay, DevInterval *__restrict__ out, uint32_t *__restrict__ counts)
+{
+  constexpr int K  = kIntervalLookahead;
+  const uint64_t r = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (r >= n)
+    return;
+  IntervalIt it;
+  intervalInit(g, depth, ld3(orgs, r), ld3(dirs, r), __ldg(tr + 2 * r), __ldg(tr + 2 * r + 1), it);
+  const float tMax = it.tMax;  // changes only when the ray ends
+  uint32_t c = 0;
+  bool live  = true;
+  while (live) {
+    const float *addr[K];
+    float tb[K], ta[K];
+    int nb = 0, budgetEnd = -1;
+    bool topEnd = false;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (nb == j && budgetEnd < 0 && !topEnd) {
+        if (!(it.dda.t <= tMax)) {
+          topEnd = true;
+        } else {
+          const uint32_t L = it.dda.level;
+          int32_t cx, cy, cz;
+          ddaCell(it.dda, L, cx, cy, cz);
+          addr[j] = denseCellRange(g, cx, cy, cz, L, attr);
+          tb[j]   = it.dda.t;
+          nb      = j + 1;
+          if (it.budget-- == 0) {
+            budgetEnd = j;
+          } else {
+            VoxelDesc d{};
+            d.level = L;
+            hddaStep(d, it.dda);
+            ta[j] = it.dda.t;
+          }
+        }
+      }
+    }
+    float v0[K], v1[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      v0[j] = v1[j] = 0.f;
+      if (j < nb && addr[j]) {
+        v0[j] = __ldg(addr[j]);
+        v1[j] = __ldg(addr[j] + 1);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (live && j < nb) {
+        const bool empty = !addr[j] || !rangesOverlap(vr, v0[j], v1[j]);
+        if ((!empty && !(tb[j] < tMax)) || j == budgetEnd) {
+          live = false;
+        } else if (!empty) {
+          if (c < maxPerRay)
+            out[r * maxPerRay + c] = DevInterval{tb[j], minx(ta[j], tMax), v0[j], v1[j], it.nominalDeltaT};
+          ++c;
+        }
+      }
+    }
+    if (topEnd)
+      live = false;
+  }
+  counts[r] = c;
+}
+
 // The ray source of the persistent hit kernels: rays first, first + stride,
 // ... below n, each with its slots out[r * maxPerRay ..] and count counts[r].
 struct StridedRays {
@@ -184,8 +265,12 @@ void launchIntervals(const DevGrid &g, uint32_t attr, uint32_t depth, DevValueRa
 {
   if (!n)
     return;
-  kIntervals<<<blocksFor(n), kBlock, 0, st>>>(g, attr, depth, vr, n, origins, directions, tRanges,
-                                               maxPerRay, out, counts);
+  if (g.dense)
+    kIntervalsDense<<<blocksFor(n), kBlock, 0, st>>>(g, attr, depth, vr, n, origins, directions, tRanges,
+                                                      maxPerRay, out, counts);
+  else
+    kIntervals<<<blocksFor(n), kBlock, 0, st>>>(g, attr, depth, vr, n, origins, directions, tRanges, maxPerRay,
+                                                 out, counts);
   cudaCheck(cudaGetLastError(), "interval kernel launch");
 }
 
