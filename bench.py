@@ -422,8 +422,9 @@ def run_patterns(args):
     (3 timed, 2 warm-up):
       compressed  2^26 points in active leaves of the 4096^3 shell VDB:
                   FP32 leaves vs FP16 / BF16 / FP8-E4M3 codes (per-leaf scale
-                  and offset), speed-up over FP32 and error against the FP64
-                  trilinear of the float leaves
+                  and offset; 512 codes per leaf, or 8 stencil blocks of 5^3
+                  codes per leaf), speed-up over FP32 and error against the
+                  FP64 trilinear of the float leaves
       batched     the 512-volume batch vs per-volume launches (eager and in
                   a CUDA graph), sample + gradient of every point
       learned     the hash-grid + MLP surrogate of the shell VDB, trained on
@@ -472,7 +473,9 @@ def run_vdb_coherent(args):
 def run_vdb(args, coherent=False):
     """Sparse VDB (4096^3 domain, ~5 % of leaves active, shells with fractal
     noise), trilinear sampleN at 2^26 points inside active leaves: plain
-    float leaves vs FP16 / BF16 / FP8-E4M3 codes with per-leaf scale+offset.
+    float leaves vs FP16 / BF16 / FP8-E4M3 codes with per-leaf scale+offset,
+    as 512 codes per leaf or as 8 stencil blocks of 5^3 codes per leaf
+    (scale and offset over the leaf's 9^3 sampling window; "_blocks").
     Errors of the compressed forms are against the float path on the same
     points, relative to the volume's value range."""
     import torch
@@ -515,7 +518,7 @@ def run_vdb(args, coherent=False):
 
     results, ref = {}, None
     vrange = float(values.max().item() - values.min().item())
-    for fmt in ("f32", "fp16", "bf16", "fp8"):
+    for fmt in ("f32", "fp16", "bf16", "fp8", "fp16_blocks", "bf16_blocks", "fp8_blocks"):
         vol, commit_s = volume(fmt)
         smp = vkl.Sampler(vol, filter=100)
         for _ in range(args.warmup):
@@ -529,7 +532,8 @@ def run_vdb(args, coherent=False):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         r = {"value": npts / (ms * 1e-3) / 1e9, "ms_per_step": ms, "commit_s": commit_s,
-             "leaf_bytes": L * 512 * {"f32": 4, "fp16": 2, "bf16": 2, "fp8": 1}[fmt]}
+             "leaf_bytes": L * {"f32": 2048, "fp16": 1024, "bf16": 1024, "fp8": 512, "fp16_blocks": 2048,
+                                "bf16_blocks": 2048, "fp8_blocks": 1024}[fmt]}
         if ref is None:
             ref = out.clone()
         else:

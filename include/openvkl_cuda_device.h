@@ -95,6 +95,12 @@ __device__ __forceinline__ auto withField(const DevGrid &g, uint32_t attr, uint3
     return f(SparseField<CodeBF16>(g, attr, depth));
   case kCompressFP8:
     return f(SparseField<CodeE4M3>(g, attr, depth));
+  case kCompressFP16Blocks:
+    return f(SparseField<Blocked<CodeFP16>>(g, attr, depth));
+  case kCompressBF16Blocks:
+    return f(SparseField<Blocked<CodeBF16>>(g, attr, depth));
+  case kCompressFP8Blocks:
+    return f(SparseField<Blocked<CodeE4M3>>(g, attr, depth));
   default:
     break;
   }

@@ -100,13 +100,32 @@ struct DevLevel {
 };
 
 // Compressed leaf storage (FP16/BF16/FP8-E4M3 with per-leaf scale+offset);
-// `format` 0 = none (plain float/half leaves).
+// `format` 0 = none (plain float/half leaves).  The *Blocks formats store
+// each leaf as 8 stencil blocks (kLeafBlock* below) instead of 512 codes.
 enum : uint32_t {
-  kCompressNone = 0,
-  kCompressFP16 = 1,
-  kCompressBF16 = 2,
-  kCompressFP8  = 3,
+  kCompressNone       = 0,
+  kCompressFP16       = 1,
+  kCompressBF16       = 2,
+  kCompressFP8        = 3,
+  kCompressFP16Blocks = 4,
+  kCompressBF16Blocks = 5,
+  kCompressFP8Blocks  = 6,
 };
+
+// Stencil-block leaves: leaf voxel (x, y, z) in [0, 8)^3 lies in block
+// ((x >> 2) << 2 | (y >> 2) << 1 | (z >> 2)); a block holds the 5^3 voxels
+// 4 * b + [0, 4] per axis (its 4^3 voxels plus the next voxel on the +x/+y/+z
+// side, which may lie in a neighbouring leaf), z fastest, padded to 128
+// codes.  A trilinear stencil whose base voxel lies in the leaf reads all 8
+// corners from one block.
+constexpr uint32_t kLeafBlockCodes = 128;
+constexpr uint32_t kLeafCodes      = 8 * kLeafBlockCodes;
+
+VKL_HD uint32_t leafBlockCode(uint32_t x, uint32_t y, uint32_t z)
+{
+  return ((((x >> 2) & 1u) << 2 | ((y >> 2) & 1u) << 1 | ((z >> 2) & 1u)) * kLeafBlockCodes) +
+         (x & 3u) * 25u + (y & 3u) * 5u + (z & 3u);
+}
 
 constexpr uint32_t kMaxLeafObservers = 4;
 

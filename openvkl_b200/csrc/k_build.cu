@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(128) kSparseLeafRanges(const __grid_constant__
       for (uint32_t x = xa; x < xb; ++x)
         for (uint32_t y = ya; y < yb; ++y)
           for (uint32_t z = za; z < zb; ++z) {
-            const float v = packedLeafValue<T>(g, attr, li, li * 512 + (x << 6) + (y << 3) + z);
+            const float v = packedLeafValue<T>(g, attr, li, leafVoxelIndex<T>(li, x, y, z));
             nlo           = fminx(nlo, v);
             nhi           = fmaxx(nhi, v);
           }
@@ -642,6 +642,90 @@ __global__ void __launch_bounds__(256) kCompressLeaves(const float *__restrict__
     encodeCode((x[i] - offset) / scale, c + lane + 32 * i);
 }
 
+// ---------------------------------------------------------------------------
+// Stencil-block leaves (extension): per dense leaf slot, the 9^3 sampling
+// window (the leaf's voxels plus the next voxel on the +x/+y/+z side, as the
+// float volume's full-depth lookup gives them: neighbouring leaves, tiles,
+// zero in empty space, background outside the domain) sets the leaf's scale
+// and offset by kCompressLeaves' rule over the window's non-NaN values, and
+// the leaf's 8 blocks of 5^3 codes are encoded from the window (block layout:
+// leafBlockCode, grid.h).  One CTA of 128 threads per slot; slots whose
+// offset is ~0 (tiles of node.data input) are skipped.
+// ---------------------------------------------------------------------------
+template <typename C>
+__global__ void __launch_bounds__(128) kBuildLeafBlocks(const __grid_constant__ DevGrid g, uint32_t attr,
+                                                        const uint32_t *__restrict__ offs, float codeMax,
+                                                        C *__restrict__ codes, float2 *__restrict__ scaleOffset)
+{
+  const uint64_t slot = blockIdx.x;
+  const uint32_t cx = offs[3 * slot], cy = offs[3 * slot + 1], cz = offs[3 * slot + 2];
+  if (cx == ~0u)
+    return;
+  __shared__ float win[729];
+  __shared__ float red[2][4];
+  const SparseField<float> F(g, attr, kNumLevels - 1);
+  const float *leaf = (const float *)g.data[attr] + slot * 512;
+  float lo = kInf, hi = -kInf;
+  for (int w = threadIdx.x; w < 729; w += 128) {
+    const uint32_t wx = w / 81, wy = (w / 9) % 9, wz = w % 9;
+    float v;
+    if (wx < 8 && wy < 8 && wz < 8)
+      v = __ldg(leaf + (wx << 6) + (wy << 3) + wz);
+    else
+      v = F.at(g.rootOrigin[0] + (int32_t)(cx + wx), g.rootOrigin[1] + (int32_t)(cy + wy),
+               g.rootOrigin[2] + (int32_t)(cz + wz));
+    win[w] = v;
+    if (v < lo)
+      lo = v;
+    if (v > hi)
+      hi = v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+    if (l2 < lo)
+      lo = l2;
+    if (h2 > hi)
+      hi = h2;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = lo;
+    red[1][threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  lo = kInf;
+  hi = -kInf;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (red[0][k] < lo)
+      lo = red[0][k];
+    if (red[1][k] > hi)
+      hi = red[1][k];
+  }
+  lo += 0.f;  // one sign for zero
+  hi += 0.f;
+  float offset = 0.f, scale = 1.f;
+  if (lo <= hi) {
+    offset           = 0.5f * lo + 0.5f * hi;
+    const float half = 0.5f * hi - 0.5f * lo;
+    if (half > 0.f)
+      scale = half / codeMax;
+  }
+  if (threadIdx.x == 0)
+    scaleOffset[slot] = make_float2(scale, offset);
+  C *c = codes + slot * kLeafCodes;
+  for (uint32_t k = threadIdx.x; k < kLeafCodes; k += 128) {
+    const uint32_t b = k / kLeafBlockCodes, l = k % kLeafBlockCodes;
+    if (l < 125) {
+      const uint32_t x = ((b >> 2) & 1u) * 4 + l / 25, y = ((b >> 1) & 1u) * 4 + (l / 5) % 5,
+                     z = (b & 1u) * 4 + l % 5;
+      encodeCode((win[x * 81 + y * 9 + z] - offset) / scale, c + k);
+    } else {
+      encodeCode(0.f, c + k);
+    }
+  }
+}
+
 inline unsigned blocksFor(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
@@ -705,6 +789,12 @@ void launchSparseLeafRanges(const DevGrid &g, uint32_t attr, uint64_t numLeaves,
     kSparseLeafRanges<CodeBF16><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
   else if (g.compress == kCompressFP8)
     kSparseLeafRanges<CodeE4M3><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.compress == kCompressFP16Blocks)
+    kSparseLeafRanges<Blocked<CodeFP16>><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.compress == kCompressBF16Blocks)
+    kSparseLeafRanges<Blocked<CodeBF16>><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
+  else if (g.compress == kCompressFP8Blocks)
+    kSparseLeafRanges<Blocked<CodeE4M3>><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
   else if (g.type[attr] == kHalf)
     kSparseLeafRanges<__half><<<grid, 128, 0, st>>>(g, attr, numLeaves, leafOffsets, leafRanges);
   else
@@ -766,6 +856,22 @@ void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves,
   else
     kCompressLeaves<<<grid, 256, 0, st>>>(src, numLeaves, 448.f, (__nv_fp8_storage_t *)codes, so);
   cudaCheck(cudaGetLastError(), "leaf compression kernel");
+}
+
+void launchBuildLeafBlocks(uint32_t format, const DevGrid &g, uint32_t attr, uint64_t numSlots,
+                           const uint32_t *slotOffsets, void *codes, float *scaleOffset, cudaStream_t st)
+{
+  if (!numSlots)
+    return;
+  const unsigned grid = (unsigned)numSlots;
+  float2 *so          = (float2 *)scaleOffset;
+  if (format == kCompressFP16Blocks)
+    kBuildLeafBlocks<<<grid, 128, 0, st>>>(g, attr, slotOffsets, 1.f, (__half *)codes, so);
+  else if (format == kCompressBF16Blocks)
+    kBuildLeafBlocks<<<grid, 128, 0, st>>>(g, attr, slotOffsets, 1.f, (__nv_bfloat16 *)codes, so);
+  else
+    kBuildLeafBlocks<<<grid, 128, 0, st>>>(g, attr, slotOffsets, 448.f, (__nv_fp8_storage_t *)codes, so);
+  cudaCheck(cudaGetLastError(), "leaf block kernel");
 }
 
 }  // namespace vklcuda

@@ -26,6 +26,11 @@ void launchBuildLeafMap(const DevGrid &g, uint64_t *map, cudaStream_t stream);
 // (scale, offset) float pair per leaf.
 void launchCompressLeaves(uint32_t format, const float *src, uint64_t numLeaves, void *codes,
                           float *scaleOffset, cudaStream_t stream);
+// Stencil-block leaves (format kCompress*Blocks): from the float volume g
+// (leaf map built), per dense slot (root-relative leaf offsets, 3 per slot,
+// ~0 for slots to skip) kLeafCodes codes and one (scale, offset) pair.
+void launchBuildLeafBlocks(uint32_t format, const DevGrid &g, uint32_t attr, uint64_t numSlots,
+                           const uint32_t *slotOffsets, void *codes, float *scaleOffset, cudaStream_t stream);
 // Element count of the bricked copy of a dense x-fastest voxel array
 // (brickIndex, grid.h) and its supertile counts.
 uint64_t brickedElements(const uint32_t dims[3], uint32_t &superX, uint32_t &superY);

@@ -955,7 +955,10 @@ void Volume::commitVdb()
   }
   // Compressed leaves (extension parameter "compression": "fp16" | "bf16" |
   // "fp8"): float packed leaves are re-encoded on the GPU with one
-  // (scale, offset) pair per leaf; tiles stay float.
+  // (scale, offset) pair per leaf; tiles stay float.  The stencil-block
+  // forms ("fp16_blocks" | "bf16_blocks" | "fp8_blocks") are encoded after
+  // the tree and leaf map exist (their blocks reach into neighbouring leaves).
+  uint32_t blockedFmt = kCompressNone;
   if (const Param *cp = find("compression")) {
     const std::string &c = cp->str;
     uint32_t fmt = kCompressNone;
@@ -965,8 +968,16 @@ void Volume::commitVdb()
       fmt = kCompressBF16;
     else if (c == "fp8" || c == "fp8_e4m3")
       fmt = kCompressFP8;
+    else if (c == "fp16_blocks")
+      blockedFmt = kCompressFP16Blocks;
+    else if (c == "bf16_blocks")
+      blockedFmt = kCompressBF16Blocks;
+    else if (c == "fp8_blocks" || c == "fp8_e4m3_blocks")
+      blockedFmt = kCompressFP8Blocks;
     else if (!(c.empty() || c == "none"))
-      fail("compression must be one of none, fp16, bf16, fp8");
+      fail("compression must be one of none, fp16, bf16, fp8, fp16_blocks, bf16_blocks, fp8_blocks");
+    if (blockedFmt != kCompressNone && leafType != VKL_FLOAT)
+      fail("compression requires VKL_FLOAT leaves");
     if (fmt != kCompressNone) {
       if (leafType != VKL_FLOAT)
         fail("compression requires VKL_FLOAT leaves");
@@ -1134,6 +1145,34 @@ void Volume::commitVdb()
     } else {
       grid.leafMapDims[0] = grid.leafMapDims[1] = grid.leafMapDims[2] = 0;
     }
+  }
+
+  if (blockedFmt != kCompressNone) {
+    // per dense slot its leaf's root-relative offset (~0: a tile's unused
+    // slot of node.data input)
+    const uint64_t slots = hasPacked ? nDense : numLeaves;
+    std::vector<uint32_t> slotOff(3 * std::max<uint64_t>(slots, 1), ~0u);
+    for (uint64_t i = 0; i < numLeaves; ++i)
+      if (formats[i] == kFormatDenseZYX) {
+        const uint64_t sl = hasPacked ? packedIndex[i] : i;
+        for (int a = 0; a < 3; ++a)
+          slotOff[3 * sl + a] = off[3 * i + a];
+      }
+    DeviceBuffer dSlotOff;
+    dSlotOff.alloc(slotOff.size() * 4);
+    cudaCheck(cudaMemcpy(dSlotOff.ptr, slotOff.data(), slotOff.size() * 4, cudaMemcpyHostToDevice), "upload");
+    const size_t codeBytes = blockedFmt == kCompressFP8Blocks ? 1 : 2;
+    const DevGrid floatGrid = grid;
+    for (uint32_t a = 0; a < grid.numAttributes; ++a) {
+      DeviceBuffer *bc = newBuffer(std::max<uint64_t>(slots, 1) * kLeafCodes * codeBytes);
+      DeviceBuffer *bs = newBuffer(std::max<uint64_t>(slots, 1) * 8);
+      launchBuildLeafBlocks(blockedFmt, floatGrid, a, slots, dSlotOff.as<uint32_t>(), bc->ptr, bs->as<float>(),
+                            device->stream);
+      grid.data[a]            = bc->ptr;
+      grid.leafScaleOffset[a] = bs->as<float>();
+    }
+    cudaCheck(cudaStreamSynchronize(device->stream), "leaf blocks");
+    grid.compress = blockedFmt;
   }
 
   DeviceBuffer dOff, dLeafVoxel, leafRanges, volRange;

@@ -279,6 +279,12 @@ void dispatchFilter(const DevGrid &g, uint32_t maxDepth, uint64_t n, const float
     return launchTyped<CodeBF16, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
   case kCompressFP8:
     return launchTyped<CodeE4M3, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  case kCompressFP16Blocks:
+    return launchTyped<Blocked<CodeFP16>, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  case kCompressBF16Blocks:
+    return launchTyped<Blocked<CodeBF16>, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
+  case kCompressFP8Blocks:
+    return launchTyped<Blocked<CodeE4M3>, false, FILTER>(g, maxDepth, n, pts, attr, out, grad, st);
   default:
     break;
   }

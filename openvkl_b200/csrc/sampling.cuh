@@ -395,31 +395,55 @@ struct AtlasField {
 struct CodeFP16 {};
 struct CodeBF16 {};
 struct CodeE4M3 {};
+// Stencil-block leaves (kLeafBlockCodes / leafBlockCode in grid.h): the
+// same codes, laid out as 8 blocks of 5^3 per leaf whose (scale, offset)
+// spans the leaf's 9^3 sampling window.
+template <class C>
+struct Blocked {};
 
 template <typename T>
 struct LeafCodec {
-  static constexpr bool kScaled = false;
-  using Tile                    = T;
-  using Code                    = T;
+  static constexpr bool kScaled  = false;
+  static constexpr bool kBlocked = false;
+  using Tile                     = T;
+  using Code                     = T;
 };
 template <>
 struct LeafCodec<CodeFP16> {
-  static constexpr bool kScaled = true;
-  using Tile                    = float;
-  using Code                    = __half;
+  static constexpr bool kScaled  = true;
+  static constexpr bool kBlocked = false;
+  using Tile                     = float;
+  using Code                     = __half;
 };
 template <>
 struct LeafCodec<CodeBF16> {
-  static constexpr bool kScaled = true;
-  using Tile                    = float;
-  using Code                    = __nv_bfloat16;
+  static constexpr bool kScaled  = true;
+  static constexpr bool kBlocked = false;
+  using Tile                     = float;
+  using Code                     = __nv_bfloat16;
 };
 template <>
 struct LeafCodec<CodeE4M3> {
-  static constexpr bool kScaled = true;
-  using Tile                    = float;
-  using Code                    = __nv_fp8_storage_t;
+  static constexpr bool kScaled  = true;
+  static constexpr bool kBlocked = false;
+  using Tile                     = float;
+  using Code                     = __nv_fp8_storage_t;
 };
+template <class C>
+struct LeafCodec<Blocked<C>> : LeafCodec<C> {
+  static constexpr bool kBlocked = true;
+};
+
+// Offset of leaf voxel (x, y, z) (low 3 bits of each used) within its
+// leaf's slot of the data array: z-fastest 8^3, or the stencil-block layout.
+template <typename T>
+__device__ __forceinline__ uint64_t leafVoxelIndex(uint64_t li, uint32_t x, uint32_t y, uint32_t z)
+{
+  if constexpr (LeafCodec<T>::kBlocked)
+    return li * kLeafCodes + leafBlockCode(x & 7u, y & 7u, z & 7u);
+  else
+    return li * 512 + ((uint64_t)(x & 7u) << 6) + ((y & 7u) << 3) + (z & 7u);
+}
 
 __device__ __forceinline__ float ldCode(const __half *p, uint64_t i)
 {
@@ -530,7 +554,7 @@ struct SparseField {
       const uint64_t li = voxelLeafIndex(voxel);
       if (voxelLeafFormat(voxel) == kFormatTile)
         return tileValue<T>(g, attr, li);
-      const uint64_t vi = li * 512 + ((uint64_t)(ox & 7u) << 6) + ((oy & 7u) << 3) + (oz & 7u);
+      const uint64_t vi = leafVoxelIndex<T>(li, ox, oy, oz);
       if constexpr (LeafCodec<T>::kScaled)
         return ldCode((const typename LeafCodec<T>::Code *)g.data[attr], vi) * so.x + so.y;
       else
@@ -569,6 +593,22 @@ struct SparseField {
     const uint32_t bx = (uint32_t)(x + LO - g.rootOrigin[0]),
                    by = (uint32_t)(y + LO - g.rootOrigin[1]),
                    bz = (uint32_t)(z + LO - g.rootOrigin[2]);
+    if constexpr (W == 2 && LeafCodec<T>::kBlocked) {
+      // Stencil-block leaves: when the base voxel lies in a dense leaf, all
+      // 8 corners are that leaf's block codes (one leaf lookup, one block).
+      if (bx < g.activeSize[0] && by < g.activeSize[1] && bz < g.activeSize[2]) {
+        const uint64_t v = traverse(bx, by, bz);
+        if (voxelIsLeaf(v) && voxelLeafFormat(v) != kFormatTile) {
+          const uint64_t li = voxelLeafIndex(v);
+          const float2 so   = __ldg((const float2 *)g.leafScaleOffset[attr] + li);
+          const auto *c     = (const typename LeafCodec<T>::Code *)g.data[attr] + leafVoxelIndex<T>(li, bx, by, bz);
+#pragma unroll
+          for (int o = 0; o < 8; ++o)
+            s[o] = ldCode(c, (o >> 2) * 25 + ((o >> 1) & 1) * 5 + (o & 1)) * so.x + so.y;
+          return;
+        }
+      }
+    }
     if constexpr (W == 2) {
       // 2^3 corners: along an axis the second corner is in the next leaf
       // only when the first sits on the leaf's last voxel.  Leaf slot s
@@ -821,6 +861,12 @@ __device__ __forceinline__ float sampleIndexAny(const DevGrid &g, int filter, ui
     return sampleFiltered(SparseField<CodeBF16>(g, attr, depth), filter, cc, p);
   case kCompressFP8:
     return sampleFiltered(SparseField<CodeE4M3>(g, attr, depth), filter, cc, p);
+  case kCompressFP16Blocks:
+    return sampleFiltered(SparseField<Blocked<CodeFP16>>(g, attr, depth), filter, cc, p);
+  case kCompressBF16Blocks:
+    return sampleFiltered(SparseField<Blocked<CodeBF16>>(g, attr, depth), filter, cc, p);
+  case kCompressFP8Blocks:
+    return sampleFiltered(SparseField<Blocked<CodeE4M3>>(g, attr, depth), filter, cc, p);
   default:
     break;
   }
@@ -871,6 +917,12 @@ __device__ __forceinline__ f3 gradientObjectAny(const DevGrid &g, int filter, ui
     return gradientFiltered(g, SparseField<CodeBF16>(g, attr, depth), filter, p);
   case kCompressFP8:
     return gradientFiltered(g, SparseField<CodeE4M3>(g, attr, depth), filter, p);
+  case kCompressFP16Blocks:
+    return gradientFiltered(g, SparseField<Blocked<CodeFP16>>(g, attr, depth), filter, p);
+  case kCompressBF16Blocks:
+    return gradientFiltered(g, SparseField<Blocked<CodeBF16>>(g, attr, depth), filter, p);
+  case kCompressFP8Blocks:
+    return gradientFiltered(g, SparseField<Blocked<CodeE4M3>>(g, attr, depth), filter, p);
   default:
     break;
   }

@@ -681,7 +681,11 @@ def vdb_volume(device: Device, levels, origins, formats, packed_dense=None, pack
     """A committed vdb volume from packed leaves (nodesPackedDense / Tile, one
     array or a list per attribute) or per-leaf node.data arrays.
     `compression` ("fp16" | "bf16" | "fp8") stores float leaves as codes with
-    a per-leaf scale and offset (cuda device extension).  `shared`: the
+    a per-leaf scale and offset (cuda device extension); "fp16_blocks" |
+    "bf16_blocks" | "fp8_blocks" store each leaf as 8 stencil blocks of 5^3
+    codes (the leaf's voxels plus the next voxel on the +x/+y/+z side, one
+    scale and offset over that 9^3 window), so a trilinear stencil based in
+    the leaf reads one block.  `shared`: the
     packed leaf arrays are VKL_DATA_SHARED_BUFFER (used in place)."""
     v = Volume(device, "vdb")
     v.set_data("node.level", Data(device, np.ascontiguousarray(levels, np.uint32)))

@@ -109,6 +109,9 @@ def lib(fast: bool = False, fma: bool = False) -> C.CDLL:
         L.orc_inner_nodes.argtypes = [P, U32, U32, U64, P]
         L.orc_round_format.argtypes = [C.c_int, U64, P, P]
         L.orc_quantize_leaves.argtypes = [C.c_int, U64, P, P, P]
+        L.orc_quantize_groups.argtypes = [C.c_int, U64, U32, P, P, P]
+        L.orc_vdb_leaf_windows.argtypes = [P, U32, P]
+        L.orc_vdb_set_windows.argtypes = [P, U32, U64, P]
         _libs[name] = L
     return _libs[name]
 
@@ -214,7 +217,22 @@ class OracleVolume:
                              pdp, ptp, _p(i2o), _p(clip), _p(bg))
         if not h:
             raise RuntimeError(L.orc_last_error().decode())
-        return OracleVolume(h, {"pd": pd, "pt": pt, "dense": False}, fast, fma)
+        return OracleVolume(h, {"pd": pd, "pt": pt, "dense": False, "formats": formats}, fast, fma)
+
+    def leaf_windows(self, attr=0):
+        """(dense leaf slots, 9, 9, 9) float32: each dense leaf's voxels plus the
+        next voxel on the +x/+y/+z side, by full-depth lookups (x outermost)."""
+        n = int(np.count_nonzero(np.asarray(self._keep["formats"]) == 1))  # VKL_FORMAT_DENSE_ZYX
+        w = np.empty((n, 9, 9, 9), np.float32)
+        self._lib.orc_vdb_leaf_windows(self._h, attr, _p(w))
+        return w
+
+    def set_windows(self, decoded, attr=0):
+        """Install decoded stencil-block windows: trilinear stencils whose base
+        voxel lies in a dense leaf then read their corners from its window."""
+        w = np.ascontiguousarray(decoded, np.float32).reshape(-1, 729)
+        self._keep.setdefault("windows", {})[attr] = w
+        self._lib.orc_vdb_set_windows(self._h, attr, w.shape[0], _p(w))
 
     # ---- introspection ------------------------------------------------
     def info(self):
@@ -421,3 +439,37 @@ def quantize_leaves(fmt, leaves):
     so = np.empty((n, 2), np.float32)
     lib().orc_quantize_leaves(COMPRESSION_FORMATS[fmt], n, _p(x), _p(dec), _p(so))
     return dec, so
+
+
+def quantize_groups(fmt, values, group):
+    """Groups of `group` floats -> (decoded floats, (n,2) scale/offset) by the
+    compressed-leaf rule (one scale and offset per group)."""
+    x = np.ascontiguousarray(values, np.float32).reshape(-1)
+    n = x.size // group
+    dec = np.empty_like(x)
+    so = np.empty((n, 2), np.float32)
+    lib().orc_quantize_groups(COMPRESSION_FORMATS[fmt], n, group, _p(x), _p(dec), _p(so))
+    return dec, so
+
+
+def vdb_blocked_volume(fmt, levels, origins, formats, packed_dense, packed_tile=None, **kw):
+    """The oracle of the cuda device's stencil-block leaves (compression
+    "<fmt>_blocks"): each dense leaf's 9^3 sampling window of the float volume
+    quantized with one scale and offset, the leaves' own voxels decoded from
+    it, and trilinear stencils based in a dense leaf read from its window.
+    Returns (volume, per-attribute (n, 2) scale/offset arrays)."""
+    flt = OracleVolume.vdb_volume(levels, origins, formats, packed_dense, packed_tile, **kw)
+    pd = packed_dense if isinstance(packed_dense, (list, tuple)) else [packed_dense]
+    wins, sos, inner = [], [], []
+    for a in range(len(pd)):
+        w = flt.leaf_windows(a)
+        dec, so = quantize_groups(fmt, w, 729)
+        dec = dec.reshape(-1, 9, 9, 9)
+        wins.append(dec)
+        sos.append(so)
+        inner.append(np.ascontiguousarray(dec[:, :8, :8, :8]).reshape(-1))
+    vol = OracleVolume.vdb_volume(levels, origins, formats, inner if len(inner) > 1 else inner[0],
+                                  packed_tile, **kw)
+    for a, w in enumerate(wins):
+        vol.set_windows(w, a)
+    return vol, sos

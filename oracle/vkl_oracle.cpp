@@ -279,6 +279,9 @@ struct Grid {
   std::vector<vec3i> leafOrigin;
   Level levels[NUM_LEVELS - 1];
   std::vector<range1f> volumeRange;
+  // stencil-block leaves (the cuda device's extension): per attribute the
+  // decoded 9^3 sampling window of every dense leaf slot (empty: off)
+  std::vector<std::vector<float>> blockWin;
 };
 
 // ---------------------------------------------------------------------------
@@ -543,6 +546,22 @@ inline void trilinearTaps(const Grid &g,
                           uint32_t d,
                           float s[8])
 {
+  // Stencil-block leaves (the cuda device's extension, no reference
+  // counterpart): a base voxel inside a dense leaf takes all 8 corners from
+  // that leaf's decoded 9^3 window.
+  if (!g.dense && a < g.blockWin.size() && !g.blockWin[a].empty()) {
+    const vec3ui o = toDomainOffset(ic, g.rootOrigin);
+    if (inDomain(g.activeSize, o)) {
+      const uint64_t v = traverse(g, o, d);
+      if (vLeaf(v) && leafFmt(v) != FMT_TILE) {
+        const float *w = &g.blockWin[a][leafIdx(v) * 729];
+        const uint32_t lx = o.x & 7u, ly = o.y & 7u, lz = o.z & 7u;
+        for (int k = 0; k < 8; ++k)
+          s[k] = w[(lx + (k >> 2)) * 81 + (ly + ((k >> 1) & 1)) * 9 + lz + (k & 1)];
+        return;
+      }
+    }
+  }
   for (int o = 0; o < 8; ++o)
     s[o] = tap(g, {ic.x + (o >> 2), ic.y + ((o >> 1) & 1), ic.z + (o & 1)}, a, d);
 }
@@ -2656,11 +2675,18 @@ void orc_round_format(int format, uint64_t n, const float *in, float *out)
 void orc_quantize_leaves(int format, uint64_t numLeaves, const float *in, float *decoded,
                          float *scaleOffset)
 {
+  orc_quantize_groups(format, numLeaves, 512, in, decoded, scaleOffset);
+}
+
+void orc_quantize_groups(int format, uint64_t numGroups, uint32_t groupSize, const float *in,
+                         float *decoded, float *scaleOffset)
+{
   const float codeMax = format == 3 ? 448.f : 1.f;
+  const uint64_t numLeaves = numGroups;
   for (uint64_t l = 0; l < numLeaves; ++l) {
-    const float *v = in + l * 512;
+    const float *v = in + l * groupSize;
     float lo = std::numeric_limits<float>::infinity(), hi = -lo;
-    for (int i = 0; i < 512; ++i) {
+    for (uint32_t i = 0; i < groupSize; ++i) {
       if (v[i] < lo)
         lo = v[i];
       if (v[i] > hi)
@@ -2677,9 +2703,37 @@ void orc_quantize_leaves(int format, uint64_t numLeaves, const float *in, float 
     }
     scaleOffset[2 * l]     = scale;
     scaleOffset[2 * l + 1] = offset;
-    for (int i = 0; i < 512; ++i) {
-      const float code       = roundFormat(format, (v[i] - offset) / scale);
-      decoded[l * 512 + i]   = code * scale + offset;
+    for (uint32_t i = 0; i < groupSize; ++i) {
+      const float code              = roundFormat(format, (v[i] - offset) / scale);
+      decoded[l * groupSize + i]    = code * scale + offset;
     }
   }
+}
+
+// Stencil-block leaves (the cuda device's extension; its kBuildLeafBlocks):
+// the 9^3 sampling window of each dense leaf slot (the leaf's voxels plus
+// the next voxel on the +x/+y/+z side) by full-depth lookups, x outermost,
+// z fastest: windows[slot * 729 + x * 81 + y * 9 + z].
+void orc_vdb_leaf_windows(const OrcVolume *v, uint32_t attr, float *windows)
+{
+  const Grid &g = v->g;
+  uint64_t slot = 0;
+  for (uint64_t i = 0; i < g.numLeaves; ++i) {
+    if (g.leafFormat[i] != FMT_DENSE_ZYX)
+      continue;
+    const vec3i o = g.leafOrigin[i];
+    float *w      = windows + slot++ * 729;
+    for (int x = 0; x < 9; ++x)
+      for (int y = 0; y < 9; ++y)
+        for (int z = 0; z < 9; ++z)
+          w[x * 81 + y * 9 + z] = traverseAndSample(g, {o.x + x, o.y + y, o.z + z}, attr, NUM_LEVELS - 1);
+  }
+}
+
+void orc_vdb_set_windows(OrcVolume *v, uint32_t attr, uint64_t numSlots, const float *decodedWindows)
+{
+  Grid &g = v->g;
+  if (g.blockWin.size() < g.numAttributes)
+    g.blockWin.resize(g.numAttributes);
+  g.blockWin[attr].assign(decodedWindows, decodedWindows + numSlots * 729);
 }

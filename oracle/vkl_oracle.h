@@ -226,6 +226,16 @@ void orc_quantize_leaves(int format,
                          const float *in,
                          float *decoded,
                          float *scaleOffset);
+// orc_quantize_groups: the same rule over groups of groupSize values.
+void orc_quantize_groups(int format, uint64_t numGroups, uint32_t groupSize, const float *in,
+                         float *decoded, float *scaleOffset);
+// Stencil-block leaves (the cuda device's extension): orc_vdb_leaf_windows
+// writes each dense leaf slot's 9^3 sampling window (full-depth lookups, x
+// outermost, z fastest); orc_vdb_set_windows installs decoded windows of an
+// attribute, whose trilinear stencils then take their 8 corners from the
+// window of the dense leaf holding the base voxel.
+void orc_vdb_leaf_windows(const OrcVolume *v, uint32_t attr, float *windows);
+void orc_vdb_set_windows(OrcVolume *v, uint32_t attr, uint64_t numSlots, const float *decodedWindows);
 
 #ifdef __cplusplus
 }

@@ -97,3 +97,67 @@ def test_compressed_error_vs_fp64(vkl, device, oracle, fmt):
     assert err_plain <= 1e-6  # the FP32 path
     assert err <= FORMATS[fmt] * 0.5 + 1e-6, (fmt, err)
     print(f"{fmt}: max |error| / value range = {err:.3e} (FP32 path {err_plain:.3e})")
+
+
+# Stencil-block leaves ("<fmt>_blocks"): each dense leaf is stored as 8
+# blocks of 5^3 codes holding its voxels plus the next voxel on the +x/+y/+z
+# side, with one scale and offset over that 9^3 window; a trilinear stencil
+# whose base voxel lies in a dense leaf reads its 8 corners from one block.
+# The oracle restates the window, the quantizer and that corner rule.
+@pytest.mark.parametrize("fmt", list(FORMATS))
+def test_blocked_vdb_bit_exact_vs_oracle(vkl, device, oracle, fmt):
+    origins, levels, formats, vals, tiles = _shells()
+    ref, _ = oracle.vdb_blocked_volume(fmt, levels, origins, formats, vals, tiles)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tiles,
+                         compression=fmt + "_blocks")
+    for level in range(3):
+        vox, rng, org = vol.tree_level(level)
+        rvox, rrng, rorg = ref.level(level, 1)
+        np.testing.assert_array_equal(vox, rvox)
+        np.testing.assert_array_equal(bits(rng), bits(rrng))
+    np.testing.assert_array_equal(vol.value_range(), ref.value_range())
+    b = ref.info()["bounds"]
+    pts = _points(origins, len(vals) // 512, b, seed=3)
+    for fv in (0, 100, 200):
+        smp = vkl.Sampler(vol, filter=fv, gradient_filter=fv)
+        np.testing.assert_array_equal(bits(smp.sample(pts)), bits(ref.sample(pts, filter=fv)))
+        np.testing.assert_array_equal(bits(smp.gradient(pts)), bits(ref.gradient(pts, filter=fv)))
+    # a depth-limited walk never reaches a leaf: the per-corner path
+    for depth in (1, 2):
+        smp = vkl.Sampler(vol, filter=100, max_sampling_depth=depth)
+        np.testing.assert_array_equal(bits(smp.sample(pts)),
+                                      bits(ref.sample(pts, filter=100, max_sampling_depth=depth)))
+    o, d, t = random_rays(1500, b[:3], b[3:], seed=4)
+    ctx = vkl.IntervalIteratorContext(vkl.Sampler(vol), value_ranges=[[0.4, 0.6]], hint=0.5)
+    got, gcnt = ctx.iterate_n(o, d, t, max_per_ray=1024)
+    want, wcnt = ref.intervals(o, d, t, value_ranges=[[0.4, 0.6]], hint=0.5, max_intervals=1024)
+    np.testing.assert_array_equal(gcnt, wcnt)
+    for r in range(len(gcnt)):
+        np.testing.assert_array_equal(bits(got[r, :gcnt[r]]), bits(want[r, :wcnt[r]]))
+    hctx = vkl.HitIteratorContext(vkl.Sampler(vol), np.array([0.25, 0.5], np.float32))
+    got, gcnt = hctx.iterate_n(o, d, t, max_per_ray=64)
+    want, wcnt = ref.hits(o, d, t, np.array([0.25, 0.5], np.float32), max_hits=64)
+    np.testing.assert_array_equal(gcnt, wcnt)
+    for r in range(len(gcnt)):
+        np.testing.assert_array_equal(bits(got[r, :gcnt[r]]), bits(want[r, :wcnt[r]]))
+    assert gcnt.sum() > 0
+
+
+@pytest.mark.parametrize("fmt", list(FORMATS))
+def test_blocked_error_vs_fp64(vkl, device, oracle, fmt):
+    """Same bound as the per-leaf codes: a window's half range is at most half
+    the value range of these volumes (no background inside the windows)."""
+    origins, levels, formats, vals, tiles = _shells(seed=6)
+    ref = oracle.OracleVolume.vdb_volume(levels, origins, formats, vals, tiles)
+    vol = vkl.vdb_volume(device, levels, origins, formats, packed_dense=vals, packed_tile=tiles,
+                         compression=fmt + "_blocks")
+    n_leaf = len(vals) // 512
+    rng = np.random.default_rng(9)
+    pts = (origins[:n_leaf][rng.integers(0, n_leaf, 50000)] + rng.uniform(0.5, 7.5, (50000, 3))).astype(np.float32)
+    exact = ref.sample_fp64(pts, filter=100)
+    got = vkl.Sampler(vol, filter=100).sample(pts).astype(np.float64)
+    ok = ~np.isnan(exact)
+    vrange = float(vals.max() - vals.min())
+    err = np.abs(got[ok] - exact[ok]).max() / vrange
+    assert err <= FORMATS[fmt] * 0.5 + 1e-6, (fmt, err)
+    print(f"{fmt}_blocks: max |error| / value range = {err:.3e}")

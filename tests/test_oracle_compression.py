@@ -77,3 +77,47 @@ def test_quantize_constant_and_nan_leaves():
         assert np.all(np.isnan(dec[1]))
         assert np.isnan(dec[2, 17]) and not np.isnan(np.delete(dec[2], 17)).any()
         assert dec[2, 0] == -1 and dec[2, -1] == 1  # the extremes decode exactly
+
+
+@pytest.mark.parametrize("fmt", ["fp16", "bf16", "fp8"])
+def test_blocked_windows_and_corner_rule(fmt):
+    """Stencil-block leaves in the oracle: each dense leaf's 9^3 window holds
+    its own voxels in [0, 8)^3 and the neighbours' (or empty space's) on the
+    +x/+y/+z side; groups of 512 quantize as whole leaves do; a stencil inside
+    one leaf reads the same decoded values through the window as through the
+    leaf, and a stencil crossing into a neighbour reads this leaf's window."""
+    from openvkl_b200.fields import shell_leaves
+    origins, values = shell_leaves(domain=64, shells=1, thickness=0.1, seed=4)
+    L = len(origins)
+    lv, fm = np.full(L, 3, np.uint32), np.ones(L, np.uint32)
+    flt = O.OracleVolume.vdb_volume(lv, origins, fm, values)
+    w = flt.leaf_windows()
+    np.testing.assert_array_equal(w[:, :8, :8, :8].reshape(L, -1), values.reshape(L, -1))
+    # the +x face of leaf 0 equals the float volume's samples at those voxels
+    face = origins[0] + np.stack(np.meshgrid([8], np.arange(9), np.arange(9), indexing="ij"), -1).reshape(-1, 3)
+    np.testing.assert_array_equal(w[0, 8].reshape(-1), flt.sample(face.astype(np.float32), filter=0))
+    d1, s1 = O.quantize_groups(fmt, values, 512)
+    d2, s2 = O.quantize_leaves(fmt, values)
+    np.testing.assert_array_equal(d1, d2)
+    np.testing.assert_array_equal(s1, s2)
+    vol, sos = O.vdb_blocked_volume(fmt, lv, origins, fm, values)
+    dec, so = O.quantize_groups(fmt, w, 729)
+    np.testing.assert_array_equal(so, sos[0])
+    dec = dec.reshape(L, 9, 9, 9)
+    rng = np.random.default_rng(2)
+    leaf = rng.integers(0, L, 4000)
+    inner = (origins[leaf] + rng.uniform(0, 7, (4000, 3))).astype(np.float32)
+    plain = O.OracleVolume.vdb_volume(lv, origins, fm, np.ascontiguousarray(dec[:, :8, :8, :8]).reshape(-1))
+    np.testing.assert_array_equal(vol.sample(inner), plain.sample(inner))
+    # base voxel on a leaf's last voxel in x: the corners come from the window
+    edge = origins[leaf].astype(np.float32) + np.float32([7.5, 3.25, 2.75])
+    f = np.float32(0.5)
+    lo, hi = dec[leaf, 7, 3:5, 2:4], dec[leaf, 8, 3:5, 2:4]
+
+    def lerp(t, a, b):
+        return (np.float32(1) - t) * a + t * b
+
+    def plane(p):
+        return lerp(np.float32(0.25), lerp(np.float32(0.75), p[:, 0, 0], p[:, 0, 1]),
+                    lerp(np.float32(0.75), p[:, 1, 0], p[:, 1, 1]))
+    np.testing.assert_array_equal(vol.sample(edge), lerp(f, plane(lo), plane(hi)))
