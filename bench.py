@@ -783,22 +783,36 @@ def run_hits(args):
         time.sleep(0.3)
         ms = _timed_device(call, args.steps, args.warmup, stream)
     total = int(cnt.to(torch.int64).sum().item())
+    # the compressed leaf forms on the same rays (a few steps each): their
+    # decoded values differ slightly, so hit counts may differ by a few
+    formats = {"f32": {"value": n / (ms * 1e-3) / 1e6, "ms_per_step": ms, "hits_per_step": total}}
+    del ctx, smp, v
+    for fmt in ("fp16", "fp16_blocks", "fp8_blocks"):
+        vf, sf, _, _, _ = _shell_sampler(dev, VDB_DOMAIN, compression=fmt)
+        cf = vkl.HitIteratorContext(sf, [0.25, 0.5])
+        callf = lambda: cf._call(cf.lib.vklIterateHitsN, C.byref(cf.h), n, go.data_ptr(), gd.data_ptr(),
+                                 gt.data_ptr(), m, out.data_ptr(), cnt.data_ptr())
+        msf = _timed_device(callf, min(args.steps, 3), min(args.warmup, 2), stream)
+        formats[fmt] = {"value": n / (msf * 1e-3) / 1e6, "ms_per_step": msf,
+                        "speedup_vs_f32": ms / msf, "hits_per_step": int(cnt.to(torch.int64).sum().item())}
+        del cf, sf, vf
     line = {"metric": METRIC, "value": n / (ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "dtype": "f32", "data": "synthetic (seeded shells + fractal noise, random rays)",
             "config": {"workload": f"hit iterator, vdb {VDB_DOMAIN}^3 domain, {L} leaves ({100 * frac:.2f} % "
                                    f"active, {shells} shells), {n} random rays, isovalues 0.25 / 0.5",
                        "rays": n, "hits_per_step": total, "leaves": L},
-            "hits_per_s": total / (ms * 1e-3),
+            "hits_per_s": total / (ms * 1e-3), "formats": formats,
             "cpu_baseline": None, "gpu_launches": args.steps, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
-def _shell_sampler(dev, domain, background=None):
+def _shell_sampler(dev, domain, background=None, compression=None):
     """The sparse VDB shell volume (nodesPackedDense, float leaves) and a
     trilinear sampler over it; returns (volume, sampler, leaf origins (L,3)
     numpy, shells, active fraction).  Without `background` the volume keeps
-    the reference's undefined (NaN) background."""
+    the reference's undefined (NaN) background; `compression` selects a
+    compressed leaf form."""
     from openvkl_b200 import fields, vkl
     origins, values, shells, frac = fields.shell_vdb_torch(domain=domain, seed=5)
     L = origins.shape[0]
@@ -809,6 +823,8 @@ def _shell_sampler(dev, domain, background=None):
     v.set_data("nodesPackedDense", vkl.Data(dev, objects=[vkl.Data(dev, values, shared=True)]))
     if background is not None:
         v.set_data("background", vkl.Data(dev, np.asarray([background], np.float32)))
+    if compression is not None:
+        v.set_string("compression", compression)
     v.commit()
     return v, vkl.Sampler(v, filter=100), origins, shells, frac
 

@@ -164,8 +164,33 @@ struct StridedRays {
 // through the out-of-line type / filter dispatch; the float trilinear ones
 // inline their field (far fewer registers, so more rays in flight per SM)
 // and look LOOKAHEAD march steps ahead.  All give the same hits.
-enum HitKind { kHitAny = 0, kHitDenseFloatLinear = 1, kHitSparseFloatLinear = 2 };
+enum HitKind {
+  kHitAny               = 0,
+  kHitDenseFloatLinear  = 1,
+  kHitSparseFloatLinear = 2,
+  kHitSparseFP16Blocks  = 3,
+  kHitSparseBF16Blocks  = 4,
+  kHitSparseFP8Blocks   = 5,
+};
 constexpr int kHitLookahead = 1;
+
+// Leaf codec of a sparse persistent hit kernel kind.
+template <int KIND>
+struct HitSparseCodec {
+  using T = float;
+};
+template <>
+struct HitSparseCodec<kHitSparseFP16Blocks> {
+  using T = Blocked<CodeFP16>;
+};
+template <>
+struct HitSparseCodec<kHitSparseBF16Blocks> {
+  using T = Blocked<CodeBF16>;
+};
+template <>
+struct HitSparseCodec<kHitSparseFP8Blocks> {
+  using T = Blocked<CodeE4M3>;
+};
 
 template <int KIND, int LOOKAHEAD>
 __global__ void __launch_bounds__(kBlock, KIND == kHitAny ? 1 : kHitMinBlocks) kHits(const __grid_constant__ DevGrid g, uint32_t attr,
@@ -202,9 +227,11 @@ __global__ void __launch_bounds__(kBlock, KIND == kHitAny ? 1 : kHitMinBlocks) k
     if constexpr (KIND == kHitDenseFloatLinear)
       hitsAllLanes(g, LinearSampleHook<DenseField<float>>{&g, DenseField<float>(g, attr)}, attr, vr, numValues,
                    values, maxPerRay, rays);
-    else
-      hitsAllLanes(g, LinearSampleHook<SparseField<float>>{&g, SparseField<float>(g, attr, kNumLevels - 1)}, attr,
-                   vr, numValues, values, maxPerRay, rays);
+    else {
+      using SF = SparseField<typename HitSparseCodec<KIND>::T>;
+      hitsAllLanes(g, LinearSampleHook<SF>{&g, SF(g, attr, kNumLevels - 1)}, attr, vr, numValues, values,
+                   maxPerRay, rays);
+    }
   }
 }
 
@@ -281,11 +308,23 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
 {
   if (!n)
     return;
-  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && g.compress == kCompressNone && !g.temporal;
+  const bool blocked = g.compress == kCompressFP16Blocks || g.compress == kCompressBF16Blocks ||
+                       g.compress == kCompressFP8Blocks;
+  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && !g.temporal &&
+                   (g.compress == kCompressNone || blocked);
   auto k         = kHits<kHitAny, 1>;
   unsigned grid  = blocksFor(n);
   if (lin) {
-    k = g.dense ? kHits<kHitDenseFloatLinear, kHitLookahead> : kHits<kHitSparseFloatLinear, kHitLookahead>;
+    if (g.dense)
+      k = kHits<kHitDenseFloatLinear, kHitLookahead>;
+    else if (g.compress == kCompressFP16Blocks)
+      k = kHits<kHitSparseFP16Blocks, kHitLookahead>;
+    else if (g.compress == kCompressBF16Blocks)
+      k = kHits<kHitSparseBF16Blocks, kHitLookahead>;
+    else if (g.compress == kCompressFP8Blocks)
+      k = kHits<kHitSparseFP8Blocks, kHitLookahead>;
+    else
+      k = kHits<kHitSparseFloatLinear, kHitLookahead>;
     // persistent: as many CTAs as are resident at once
     int dev = 0, sms = 0, perSM = 0;
     cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
