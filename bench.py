@@ -213,6 +213,25 @@ def cpu_baseline(vox, workload, budget_s=15.0):
                       f"threads, {dt:.1f} s"}
 
 
+def oracle_check(vox, workload, pts, got):
+    """Bitwise comparison of the timed run's results at a strided subset of
+    its points with the oracle (the same volume and points, all host
+    threads; NaN counts equal to NaN)."""
+    from oracle import pyoracle as O
+    f = FILTER[workload]
+    v = O.OracleVolume.dense_volume(vox, fast=True)
+    t = time.perf_counter()
+    if workload == "gradient":
+        want = v.gradient_parallel(pts, filter=f)
+    else:
+        want = v.sample_parallel(pts, filter=f)
+    a = np.ascontiguousarray(got, np.float32).reshape(-1)
+    b = np.ascontiguousarray(want, np.float32).reshape(-1)
+    same = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+    return {"points": int(len(pts)), "stride": 1021, "bit_exact": bool(same.all()),
+            "mismatches": int((~same).sum()), "oracle_s": round(time.perf_counter() - t, 2)}
+
+
 # ---------------------------------------------------------------------------
 # Runs.
 # ---------------------------------------------------------------------------
@@ -374,6 +393,12 @@ def run_cuda(args):
                "d2h_bytes_per_step": int(ho.numel()) * 4}
         del hp, ho
 
+    # a strided subset of the last timed step's results, checked against the
+    # oracle below (every 1021st point: ~520k of the coherent set)
+    chk_idx = torch.arange(0, n, 1021, device="cuda")
+    chk_pts = pts[chk_idx].cpu().numpy()
+    chk_out = out[chk_idx].cpu().numpy()
+
     patterns = None
     if rank == 0 and ws == 1 and args.workload == "coherent" and not args.no_patterns:
         # the configs' other patterns, measured after the headline in the
@@ -388,6 +413,7 @@ def run_cuda(args):
     if rank == 0:
         clocks = clk.summary()
         base = None if args.no_cpu_baseline else cpu_baseline(vox, args.workload)
+        check = None if args.no_cpu_baseline else oracle_check(vox, args.workload, chk_pts, chk_out)
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
@@ -406,7 +432,7 @@ def run_cuda(args):
             # per step: the layout detection (kDetectRuns) and the sampling
             # kernel for trilinear calls; the sampling kernel alone for tricubic
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps * (1 if f == 200 else 2),
-            "clocks": clocks,
+            "clocks": clocks, "check": check,
         }
         if patterns is not None:
             line["patterns"] = patterns

@@ -593,22 +593,6 @@ struct SparseField {
     const uint32_t bx = (uint32_t)(x + LO - g.rootOrigin[0]),
                    by = (uint32_t)(y + LO - g.rootOrigin[1]),
                    bz = (uint32_t)(z + LO - g.rootOrigin[2]);
-    if constexpr (W == 2 && LeafCodec<T>::kBlocked) {
-      // Stencil-block leaves: when the base voxel lies in a dense leaf, all
-      // 8 corners are that leaf's block codes (one leaf lookup, one block).
-      if (bx < g.activeSize[0] && by < g.activeSize[1] && bz < g.activeSize[2]) {
-        const uint64_t v = traverse(bx, by, bz);
-        if (voxelIsLeaf(v) && voxelLeafFormat(v) != kFormatTile) {
-          const uint64_t li = voxelLeafIndex(v);
-          const float2 so   = __ldg((const float2 *)g.leafScaleOffset[attr] + li);
-          const auto *c     = (const typename LeafCodec<T>::Code *)g.data[attr] + leafVoxelIndex<T>(li, bx, by, bz);
-#pragma unroll
-          for (int o = 0; o < 8; ++o)
-            s[o] = ldCode(c, (o >> 2) * 25 + ((o >> 1) & 1) * 5 + (o & 1)) * so.x + so.y;
-          return;
-        }
-      }
-    }
     if constexpr (W == 2) {
       // 2^3 corners: along an axis the second corner is in the next leaf
       // only when the first sits on the leaf's last voxel.  Leaf slot s
@@ -619,13 +603,27 @@ struct SparseField {
       const bool inx[2] = {bx < g.activeSize[0], bx + 1 < g.activeSize[0]};
       const bool iny[2] = {by < g.activeSize[1], by + 1 < g.activeSize[1]};
       const bool inz[2] = {bz < g.activeSize[2], bz + 1 < g.activeSize[2]};
+      const uint64_t base = (inx[0] && iny[0] && inz[0]) ? traverse(bx, by, bz) : 0ull;
+      if constexpr (LeafCodec<T>::kBlocked) {
+        // Stencil-block leaves: when the base voxel lies in a dense leaf, all
+        // 8 corners are that leaf's block codes (one leaf lookup, one block).
+        if (voxelIsLeaf(base) && voxelLeafFormat(base) != kFormatTile) {
+          const uint64_t li = voxelLeafIndex(base);
+          const float2 so   = __ldg((const float2 *)g.leafScaleOffset[attr] + li);
+          const auto *c     = (const typename LeafCodec<T>::Code *)g.data[attr] + leafVoxelIndex<T>(li, bx, by, bz);
+#pragma unroll
+          for (int o = 0; o < 8; ++o)
+            s[o] = ldCode(c, (o >> 2) * 25 + ((o >> 1) & 1) * 5 + (o & 1)) * so.x + so.y;
+          return;
+        }
+      }
       uint64_t code[8];
       float2 sc[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
         const bool need = (!i || cx) && (!j || cy) && (!k || cz) && inx[i] && iny[j] && inz[k];
-        code[q] = need ? traverse(bx + i, by + j, bz + k) : 0ull;
+        code[q] = q == 0 ? base : (need ? traverse(bx + i, by + j, bz + k) : 0ull);
         sc[q]   = need ? leafScale(code[q]) : make_float2(1.f, 0.f);
       }
 #pragma unroll
