@@ -171,6 +171,9 @@ enum HitKind {
   kHitSparseFP16Blocks  = 3,
   kHitSparseBF16Blocks  = 4,
   kHitSparseFP8Blocks   = 5,
+  kHitSparseFP16        = 6,
+  kHitSparseBF16        = 7,
+  kHitSparseFP8         = 8,
 };
 constexpr int kHitLookahead = 1;
 
@@ -190,6 +193,18 @@ struct HitSparseCodec<kHitSparseBF16Blocks> {
 template <>
 struct HitSparseCodec<kHitSparseFP8Blocks> {
   using T = Blocked<CodeE4M3>;
+};
+template <>
+struct HitSparseCodec<kHitSparseFP16> {
+  using T = CodeFP16;
+};
+template <>
+struct HitSparseCodec<kHitSparseBF16> {
+  using T = CodeBF16;
+};
+template <>
+struct HitSparseCodec<kHitSparseFP8> {
+  using T = CodeE4M3;
 };
 
 template <int KIND, int LOOKAHEAD>
@@ -308,10 +323,7 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
 {
   if (!n)
     return;
-  const bool blocked = g.compress == kCompressFP16Blocks || g.compress == kCompressBF16Blocks ||
-                       g.compress == kCompressFP8Blocks;
-  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && !g.temporal &&
-                   (g.compress == kCompressNone || blocked);
+  const bool lin = filter == kFilterLinear && g.type[attr] == kFloat && !g.temporal;
   auto k         = kHits<kHitAny, 1>;
   unsigned grid  = blocksFor(n);
   if (lin) {
@@ -323,6 +335,12 @@ void launchHits(const DevGrid &g, uint32_t attr, int filter, uint32_t depth, Dev
       k = kHits<kHitSparseBF16Blocks, kHitLookahead>;
     else if (g.compress == kCompressFP8Blocks)
       k = kHits<kHitSparseFP8Blocks, kHitLookahead>;
+    else if (g.compress == kCompressFP16)
+      k = kHits<kHitSparseFP16, kHitLookahead>;
+    else if (g.compress == kCompressBF16)
+      k = kHits<kHitSparseBF16, kHitLookahead>;
+    else if (g.compress == kCompressFP8)
+      k = kHits<kHitSparseFP8, kHitLookahead>;
     else
       k = kHits<kHitSparseFloatLinear, kHitLookahead>;
     // persistent: as many CTAs as are resident at once

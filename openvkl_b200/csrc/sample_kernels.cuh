@@ -112,11 +112,16 @@ __device__ __forceinline__ void tileScan(int *hist)
 // 1024^3 workload).  The texture-atlas instances are held to four (64
 // registers): they are bound by gather latency, and the fourth CTA gives
 // 90.7 vs 84 Gsamples/s on the coherent workload (16.6 vs 17.5 on random
-// points).
+// points).  The sparse (VDB) instances are held to three (85 registers, no
+// spills; 2 CTAs at 86-118 registers otherwise): on orbit-camera rays over
+// the 4096^3 shells the compressed leaf forms gain 24-35 % (stencil blocks
+// 13.7 -> 17.0 Gsamples/s), float leaves stay at 19.9-20.0, random
+// interior points move by -3 % (float, stencil blocks) to +6 % (per-leaf
+// codes).
 // ATLAS: a dense float attribute's corners come from its texture atlas
 // (AtlasField, trilinear only).
 template <typename T, bool DENSE, int FILTER, bool GRAD, int TILE, bool ATLAS = false>
-__global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : (ATLAS ? 4 : 1))
+__global__ void __launch_bounds__(kTileThreads, FILTER == kFilterCubic ? 2 : (ATLAS ? 4 : (DENSE ? 1 : 3)))
     kSampleTile(const __grid_constant__ DevGrid g, uint32_t maxDepth, uint64_t n, const float *__restrict__ pts,
                 uint32_t attr, float *__restrict__ out)
 {
