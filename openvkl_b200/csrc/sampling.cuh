@@ -369,11 +369,26 @@ struct AtlasField {
     const bool vx0 = ox < ax, vx1 = ox + 1u < ax, vy0 = oy < ay, vy1 = oy + 1u < ay, vz0 = oz < az,
                vz1 = oz + 1u < az;
     // footprint origin inside the plane's tile: (ox, oy) when valid, else
-    // (-1, -1) relative (only the +1 corner can be in the domain then)
-    const float fx = vx0 ? (float)(ox + 1u) : 0.f, fy = vy0 ? (float)(oy + 1u) : 0.f;
+    // (-1, -1) relative (only the +1 corner can be in the domain then).  The
+    // texel coordinates are integers below 2^24 (texture rows are at most
+    // 2^17 texels), so summing them as integers and converting once gives
+    // the same floats as converting the parts.
+    const uint32_t ux = vx0 ? ox + 1u : 0u, uy = vy0 ? oy + 1u : 0u;
     const uint32_t z0 = vz0 ? oz : 0u, z1 = vz1 ? oz + 1u : 0u;
-    const float4 a = tld4Red(tex, (float)((z0 & planeMask) * ax) + fx, (float)((z0 >> planeShift) * ay) + fy);
-    const float4 b = tld4Red(tex, (float)((z1 & planeMask) * ax) + fx, (float)((z1 >> planeShift) * ay) + fy);
+    const float4 a = tld4Red(tex, (float)((z0 & planeMask) * ax + ux), (float)((z0 >> planeShift) * ay + uy));
+    const float4 b = tld4Red(tex, (float)((z1 & planeMask) * ax + ux), (float)((z1 >> planeShift) * ay + uy));
+    if (vx0 & vx1 & vy0 & vy1 & vz0 & vz1) {
+      // every corner in the domain (all but the volume's outer shell)
+      s[0] = a.w;
+      s[1] = b.w;
+      s[2] = a.x;
+      s[3] = b.x;
+      s[4] = a.z;
+      s[5] = b.z;
+      s[6] = a.y;
+      s[7] = b.y;
+      return;
+    }
     s[0] = (vx0 & vy0 & vz0) ? a.w : bg;
     s[1] = (vx0 & vy0 & vz1) ? b.w : bg;
     s[2] = (vx0 & vy1 & vz0) ? a.x : bg;
